@@ -1,0 +1,126 @@
+/*
+ * wap.h - C ABI of the B200 multislice library (libwap.so).
+ *
+ * Replaces the device work of the reference's Python multislice path
+ * (wide_angle_propagation/propagation.py).  Plain pointers and sizes only:
+ * every array argument is a CUDA device pointer unless stated otherwise,
+ * complex arrays are interleaved (re, im) float32 ("complex64") or float64
+ * ("complex128") in C order, and `stream` is a cudaStream_t passed as void*.
+ * All calls are stream-ordered and return 0 on success or a negative
+ * WAP_ERR_* code; wap_last_error() gives the message of the calling thread's
+ * last failure.  Nothing allocated by the caller is freed by the library and
+ * vice versa.  A plan is not thread-safe: use one plan per host thread.
+ */
+#ifndef WAP_H_
+#define WAP_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WAP_OK 0
+#define WAP_ERR_ARG (-1)          /* bad argument (null pointer, size, ...) */
+#define WAP_ERR_UNSUPPORTED (-2)  /* grid size the kernels do not implement */
+#define WAP_ERR_CUDA (-3)         /* CUDA runtime error */
+#define WAP_ERR_TIMEOUT (-4)      /* device-side bounded wait expired */
+
+#define WAP_OP_FRESNEL_AS 0       /* simulate_fresnel_as path */
+#define WAP_OP_WPM 1              /* simulate_wpm path */
+
+#define WAP_TF_FRESNEL 0          /* fresnel_propagation_kernel */
+#define WAP_TF_ANGULAR 1          /* angular_spectrum_propagation_kernel */
+
+typedef struct wap_plan wap_plan;
+
+/* Version / build information string. */
+const char* wap_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* wap_last_error(void);
+
+/* Create a plan for ny x nx grids (powers of two, 32..2048 per axis) and up
+ * to max_batch probes per call.  op is WAP_OP_*; n_bins is the WPM bin count
+ * (ignored for WAP_OP_FRESNEL_AS).  Allocates twiddle tables and, for WPM,
+ * the per-probe reference-field workspace on the current device.
+ * Replaces the per-call setup implicit in propagation.py:305 / :358. */
+int wap_plan_create(wap_plan** plan, int ny, int nx, int max_batch, int op, int n_bins);
+
+/* Release a plan and everything it allocated. */
+int wap_plan_destroy(wap_plan* plan);
+
+/* FFT launch shape of the row pass (elements per thread) and column pass
+ * (elements per thread, columns per CTA); set by the autotuner. */
+int wap_plan_set_config(wap_plan* plan, int row_e, int col_e, int col_w);
+int wap_plan_get_config(const wap_plan* plan, int* row_e, int* col_e, int* col_w);
+
+/* Transfer function on the device, evaluated in float64.
+ *   WAP_TF_FRESNEL: propagation.py:139-145
+ *       H[i,j] = exp(i 2 pi z/lam) exp(-i pi lam z (fx_i^2 + fy_j^2))
+ *   WAP_TF_ANGULAR: propagation.py:148-156
+ *       H[i,j] = exp(i 2 pi z sqrt_c(1/lam^2 - fx_i^2 - fy_j^2))
+ * with fx = fftfreq(n, ps0), fy = fftfreq(m, ps1) (meshgrid 'ij', shape n x m).
+ * out is complex128 when out_c128 != 0, else complex64. */
+int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double z,
+                          double energy, void* out, int out_c128, void* stream);
+
+/* Fresnel / angular-spectrum multislice forward, propagation.py:305-352.
+ *   V        (n_draws, n_slices, ny, nx) float32 mean potential per slice [V]
+ *   draw     (n_probes) int32 potential draw of each probe, or NULL (all 0)
+ *   psi0     complex64 initial wave: (n_probes, ny, nx) if psi0_per_probe,
+ *            else one (ny, nx) probe shared by all
+ *   positions(n_probes, 2) int32 probe centres (row, col) applied like
+ *            move_probe (propagation.py:263-276), or NULL (no shift)
+ *   H        (ny, nx) complex64 transfer function
+ *   exit     (n_probes, ny, nx) complex64 out (also the working buffer)
+ *   dp       (n_probes, ny, nx) float32 |fftshift(fft2(exit))|^2, or NULL
+ *   stack    (n_probes, n_slices, ny, nx) complex64 wave after every slice,
+ *            or NULL (the reference always stacks; NULL skips those writes)
+ */
+int wap_multislice_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
+                       const int32_t* draw, const float* psi0, int n_probes,
+                       int psi0_per_probe, const int32_t* positions, const float* H,
+                       double dz, double energy, float* exit, float* dp, float* stack,
+                       void* stream);
+
+/* WPM adaptive-binning multislice forward, propagation.py:358-387 with the
+ * step of propagation.py:215-256 (n_bins reference indices spaced
+ * n_min + (n_max - n_min) t^power_spacing per slice, smoothstep blend of the
+ * two bracketing fields).  sampling = (dy, dx) as the reference's `ps`.
+ * Arguments otherwise as wap_multislice_fwd; n_bins must equal the plan's. */
+int wap_wpm_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
+                const int32_t* draw, const float* psi0, int n_probes, int psi0_per_probe,
+                const int32_t* positions, double dz, double energy, double sampling_y,
+                double sampling_x, double power_spacing, float* exit, float* dp,
+                float* stack, void* stream);
+
+/* Gradient of a loss of the Fresnel/AS multislice w.r.t. the potential.
+ * No counterpart function in the reference, whose paper claims autodiff
+ * through JAX (Paper/main.tex:271-274); this is the hand-written adjoint.
+ *   exit       (n_probes, ny, nx) forward exit waves (from wap_multislice_fwd)
+ *   ckpt       (n_probes, ceil(n_slices/ckpt_every), ny, nx) complex64 waves
+ *              entering slices 0, k, 2k, ... (from wap_multislice_fwd_ckpt)
+ *   grad_dp    (n_probes, ny, nx) float32 dL/d(dp), or NULL
+ *   grad_exit  (n_probes, ny, nx) complex64 torch-convention gradient of the
+ *              exit wave (dL/dRe + i dL/dIm), or NULL
+ *   grad_V     (n_draws, n_slices, ny, nx) float32 out, accumulated (+=)
+ *   work       complex64 workspace of (n_probes, ckpt_every + 2, ny, nx)
+ */
+int wap_multislice_fwd_ckpt(wap_plan* plan, const float* V, int n_slices, int n_draws,
+                            const int32_t* draw, const float* psi0, int n_probes,
+                            int psi0_per_probe, const int32_t* positions, const float* H,
+                            double dz, double energy, float* exit, float* dp, float* ckpt,
+                            int ckpt_every, void* stream);
+
+int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
+                       const int32_t* draw, int n_probes, const float* H, double dz,
+                       double energy, const float* exit, const float* ckpt, int ckpt_every,
+                       const float* grad_dp, const float* grad_exit, float* grad_V,
+                       float* work, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAP_H_ */

@@ -1,0 +1,86 @@
+"""ctypes binding of libwap.so (the C ABI declared in include/wap.h).
+
+The shared library is built in-tree (``python -m wideanglepropagation_b200.build``
+or ``__graft_entry__.build()``).  There is no fallback: if the library is
+missing or cannot be loaded, every compute entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwap.so")
+
+WAP_OK = 0
+WAP_ERR_ARG = -1
+WAP_ERR_UNSUPPORTED = -2
+WAP_ERR_CUDA = -3
+WAP_ERR_TIMEOUT = -4
+
+WAP_OP_FRESNEL_AS = 0
+WAP_OP_WPM = 1
+WAP_TF_FRESNEL = 0
+WAP_TF_ANGULAR = 1
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+# name -> (restype, argtypes); mirrors include/wap.h
+SIGNATURES = {
+    "wap_version": (ctypes.c_char_p, []),
+    "wap_last_error": (ctypes.c_char_p, []),
+    "wap_plan_create": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I, _I]),
+    "wap_plan_destroy": (_I, [_P]),
+    "wap_plan_set_config": (_I, [_P, _I, _I, _I]),
+    "wap_plan_get_config": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "wap_transfer_function": (_I, [_I, _I, _I, _D, _D, _D, _D, _P, _I, _P]),
+    "wap_multislice_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _D, _D, _P, _P, _P, _P]),
+    "wap_wpm_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P]),
+    "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
+    "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class WapError(RuntimeError):
+    """A CUDA-side failure reported by libwap.so."""
+
+
+def lib():
+    """Load libwap.so once; raise if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"libwap.so not found at {LIB_PATH}; build it with "
+                    "`python -m wideanglepropagation_b200.build` (the multislice path "
+                    "has no CPU fallback)")
+            h = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(h, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = h
+    return _lib
+
+
+def check(rc: int) -> None:
+    """Translate a WAP_* status into the reference's Python exception types."""
+    if rc == WAP_OK:
+        return
+    msg = lib().wap_last_error().decode(errors="replace")
+    if rc in (WAP_ERR_ARG, WAP_ERR_UNSUPPORTED):
+        raise ValueError(msg)
+    raise WapError(f"libwap error {rc}: {msg}")
+
+
+def version() -> str:
+    return lib().wap_version().decode()

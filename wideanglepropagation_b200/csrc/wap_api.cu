@@ -1,0 +1,591 @@
+// C ABI of libwap.so: plans, dispatch of the multislice passes, transfer
+// functions.  See include/wap.h for the contract of every entry point.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/wap.h"
+#include "wap_internal.h"
+#include "wap_passes.cuh"
+
+namespace wap {
+
+// ----------------------------------------------------------------------------
+// errors
+// ----------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(WAP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void clear_error() { g_err.clear(); }
+const char* last_error() { return g_err.c_str(); }
+
+// ----------------------------------------------------------------------------
+// physics scalars (propagation.py:14-81), float64 on the host
+// ----------------------------------------------------------------------------
+Physics physics(double energy, double dz) {
+  const double h = 6.626070040e-34, c = 299792458.0, me = 9.10938356e-31, e = 1.6021766208e-19;
+  Physics p;
+  p.e0 = me * c * c / e;
+  p.lambda = h * c / std::sqrt(energy * (2 * me * c * c / e + energy)) / e * 1.0e10;
+  p.ri_a = 2 * p.e0 + 2 * energy;
+  p.ri_inv_den = 1.0 / (energy * (2 * p.e0 + energy));
+  p.kphase = 2 * M_PI * dz / p.lambda;
+  p.k0 = 2 * M_PI / p.lambda;
+  p.e_plus_e0 = energy + p.e0;
+  return p;
+}
+
+// ----------------------------------------------------------------------------
+// twiddle tables: per Stockham stage s >= 1, W_{L R}^{j k} laid out [j][k],
+// from float64 sin/cos rounded once to float32
+// ----------------------------------------------------------------------------
+std::vector<float2> twiddle_table(int n, int e) {
+  const PlanShape p = make_plan_shape(n, e);
+  std::vector<float2> tw(p.tw_size(), make_float2(1.f, 0.f));
+  for (int s = 1; s < p.stages; ++s) {
+    const int R = p.radix(s), L = p.span(s), off = p.tw_offset(s);
+    const long long LR = (long long)L * R;
+    for (int j = 0; j < R; ++j)
+      for (int k = 0; k < L; ++k) {
+        const long long m = ((long long)j * k) % LR;
+        const double ang = -2.0 * M_PI * (double)m / (double)LR;
+        tw[off + j * L + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+      }
+  }
+  return tw;
+}
+
+// ----------------------------------------------------------------------------
+// launch helpers: one template instance per (size, elements per thread)
+// ----------------------------------------------------------------------------
+template <class K>
+static cudaError_t prep_smem(K kern, size_t smem) {
+  if (smem > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+template <int N, int E>
+size_t row_smem_bytes(int rows, int extra_bytes) {
+  return (size_t)rows * RowCfg<N, E>::PADN * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float2) + extra_bytes;
+}
+
+template <int N, int E>
+size_t col_smem_bytes(int w, int extra_bytes) {
+  return (size_t)N * w * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float2) + extra_bytes;
+}
+
+template <int N, int E>
+static cudaError_t launch_row_t(const RowArgs& a, int nb, int rows, cudaStream_t st) {
+  const size_t smem = row_smem_bytes<N, E>(rows, 0);
+  cudaError_t err = prep_smem(row_pass_kernel<N, E>, smem);
+  if (err != cudaSuccess) return err;
+  row_pass_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N, int E>
+static cudaError_t launch_col_t(const ColArgs& a, int nb, int w, cudaStream_t st) {
+  const size_t smem = col_smem_bytes<N, E>(w, 0);
+  cudaError_t err = prep_smem(col_pass_kernel<N, E>, smem);
+  if (err != cudaSuccess) return err;
+  col_pass_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N, int E>
+static cudaError_t launch_wpm_col_t(const WpmColArgs& a, int nb, int w, cudaStream_t st) {
+  const size_t smem = col_smem_bytes<N, E>(w, a.K * (int)sizeof(float));
+  cudaError_t err = prep_smem(wpm_col_kernel<N, E>, smem);
+  if (err != cudaSuccess) return err;
+  wpm_col_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int N, int E>
+static cudaError_t launch_wpm_row_t(const WpmRowArgs& a, int nb, int rows, cudaStream_t st) {
+  const int extra = a.K * (int)sizeof(float) + ((a.K + 31) / 32) * (int)sizeof(unsigned);
+  const size_t smem = row_smem_bytes<N, E>(rows, extra);
+  cudaError_t err = prep_smem(wpm_row_kernel<N, E>, smem);
+  if (err != cudaSuccess) return err;
+  wpm_row_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+#define WAP_SIZE_CASES(M, E) \
+  M(32, E) M(64, E) M(128, E) M(256, E) M(512, E) M(1024, E) M(2048, E)
+
+#define WAP_DISPATCH(FN, n, e, ...)                                     \
+  do {                                                                  \
+    switch ((e) * 100000 + (n)) {                                       \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 8)                                  \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 16)                                 \
+      default: return cudaErrorInvalidValue;                            \
+    }                                                                   \
+  } while (0)
+
+#define WAP_CASE_row(N, E) case E * 100000 + N: return launch_row_t<N, E>(a, nb, k, st);
+#define WAP_CASE_col(N, E) case E * 100000 + N: return launch_col_t<N, E>(a, nb, k, st);
+#define WAP_CASE_wcol(N, E) case E * 100000 + N: return launch_wpm_col_t<N, E>(a, nb, k, st);
+#define WAP_CASE_wrow(N, E) case E * 100000 + N: return launch_wpm_row_t<N, E>(a, nb, k, st);
+
+cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(row, n, e); }
+cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(col, n, e); }
+cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wcol, n, e); }
+cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wrow, n, e); }
+
+bool size_supported(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0; }
+
+// rows per row-type CTA: fill kRowThreads, at most the grid height
+int rows_per_cta(int nx, int e, int ny) {
+  const int T = nx / e;
+  int rows = kRowThreads / T;
+  if (rows < 1) rows = 1;
+  if (rows > ny) rows = ny;
+  return rows;
+}
+
+// ----------------------------------------------------------------------------
+// transfer functions in float64 (propagation.py:102-107, :139-156, :224-228)
+// ----------------------------------------------------------------------------
+struct TfArgs {
+  int kind, n, m, c128;
+  double ps0, ps1, z, lambda;
+  void* out;
+};
+
+// out[i, j], i < n (axis 0, fftfreq(n, ps0)), j < m (axis 1, fftfreq(m, ps1))
+__global__ void transfer_kernel(const TfArgs a) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)a.n * a.m) return;
+  const int i = (int)(idx / a.m), j = (int)(idx % a.m);
+  const double fx = fftfreq_d(i, a.n, a.ps0), fy = fftfreq_d(j, a.m, a.ps1);
+  double re, im;
+  if (a.kind == WAP_TF_FRESNEL) {
+    // exp(i 2 pi z / lam) * exp(-i pi lam z (fx^2 + fy^2)), as two factors
+    double s1, c1, s2, c2;
+    sincos(2.0 * M_PI / a.lambda * a.z, &s1, &c1);
+    sincos(-M_PI * a.lambda * a.z * (fx * fx + fy * fy), &s2, &c2);
+    re = c1 * c2 - s1 * s2;
+    im = c1 * s2 + s1 * c2;
+  } else {
+    const double q = 1.0 / (a.lambda * a.lambda) - fx * fx - fy * fy;
+    if (q >= 0.0) {
+      sincos(2.0 * M_PI * a.z * sqrt(q), &im, &re);
+    } else {
+      re = exp(-2.0 * M_PI * a.z * sqrt(-q));
+      im = 0.0;
+    }
+  }
+  if (a.c128) {
+    reinterpret_cast<double2*>(a.out)[idx] = make_double2(re, im);
+  } else {
+    reinterpret_cast<float2*>(a.out)[idx] = make_float2((float)re, (float)im);
+  }
+}
+
+}  // namespace wap
+
+using namespace wap;
+
+// ----------------------------------------------------------------------------
+// plan
+// ----------------------------------------------------------------------------
+static int upload_twiddles(wap_plan* p) {
+  for (int which = 0; which < 2; ++which) {
+    const int n = which == 0 ? p->nx : p->ny;
+    const int e = which == 0 ? p->row_e : p->col_e;
+    std::vector<float2> h = twiddle_table(n, e);
+    float2*& d = which == 0 ? p->tw_row : p->tw_col;
+    if (d) cudaFree(d);
+    d = nullptr;
+    cudaError_t err = cudaMalloc(&d, h.size() * sizeof(float2));
+    if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(twiddles)");
+    err = cudaMemcpy(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaMemcpy(twiddles)");
+  }
+  return WAP_OK;
+}
+
+static int default_col_w(int ny, int e, int nx) {
+  const int T = ny / e;
+  int w = 16;
+  while (w > 1 && (w * T > kColThreads || (size_t)ny * w * 8 > 96 * 1024)) w >>= 1;
+  if (w > nx) w = nx;
+  return w;
+}
+
+static bool config_valid(const wap_plan* p, int row_e, int col_e, int col_w) {
+  if ((row_e != 8 && row_e != 16) || (col_e != 8 && col_e != 16)) return false;
+  if (p->nx / row_e > kRowThreads) return false;
+  if (col_w < 1 || (col_w & (col_w - 1)) || col_w > p->nx) return false;
+  if (col_w * (p->ny / col_e) > kColThreads) return false;
+  if ((size_t)p->ny * col_w * 8 > 160 * 1024) return false;
+  return true;
+}
+
+extern "C" {
+
+const char* wap_version(void) { return "wap-b200 0.1 (sm_100a)"; }
+
+const char* wap_last_error(void) { return wap::last_error(); }
+
+int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n_bins) {
+  clear_error();
+  if (!out) return fail(WAP_ERR_ARG, "plan pointer is NULL");
+  *out = nullptr;
+  if (!size_supported(ny) || !size_supported(nx))
+    return fail(WAP_ERR_UNSUPPORTED, "unsupported grid %d x %d: each axis must be a power of two in [32, 2048]", ny, nx);
+  if (max_batch < 1) return fail(WAP_ERR_ARG, "max_batch must be >= 1 (got %d)", max_batch);
+  if (op != WAP_OP_FRESNEL_AS && op != WAP_OP_WPM) return fail(WAP_ERR_ARG, "unknown op %d", op);
+  if (op == WAP_OP_WPM && (n_bins < 2 || n_bins > 4096))
+    return fail(WAP_ERR_ARG, "n_bins must be in [2, 4096] (got %d)", n_bins);
+  wap_plan* p = new wap_plan();
+  cudaGetDevice(&p->device);
+  p->ny = ny;
+  p->nx = nx;
+  p->max_batch = max_batch;
+  p->op = op;
+  p->n_bins = op == WAP_OP_WPM ? n_bins : 0;
+  p->row_e = nx >= 64 ? 16 : 8;
+  p->col_e = ny >= 64 ? 16 : 8;
+  p->col_w = default_col_w(ny, p->col_e, nx);
+  int rc = upload_twiddles(p);
+  if (rc != WAP_OK) {
+    wap_plan_destroy(p);
+    return rc;
+  }
+  if (op == WAP_OP_WPM) {
+    const size_t plane = (size_t)ny * nx;
+    cudaError_t err = cudaMalloc(&p->fields, (size_t)max_batch * n_bins * plane * sizeof(float2));
+    if (err == cudaSuccess) err = cudaMalloc(&p->dpbuf, (size_t)max_batch * plane * sizeof(float2));
+    if (err == cudaSuccess) err = cudaMalloc(&p->hvac, plane * sizeof(float2));
+    if (err == cudaSuccess) err = cudaMalloc(&p->ky2, ny * sizeof(float));
+    if (err == cudaSuccess) err = cudaMalloc(&p->kx2, nx * sizeof(float));
+    if (err != cudaSuccess) {
+      wap_plan_destroy(p);
+      return cuda_fail(err, "cudaMalloc(WPM workspace)");
+    }
+  }
+  *out = p;
+  return WAP_OK;
+}
+
+int wap_plan_destroy(wap_plan* p) {
+  clear_error();
+  if (!p) return WAP_OK;
+  cudaFree(p->tw_row);
+  cudaFree(p->tw_col);
+  cudaFree(p->fields);
+  cudaFree(p->dpbuf);
+  cudaFree(p->hvac);
+  cudaFree(p->ky2);
+  cudaFree(p->kx2);
+  cudaFree(p->refs);
+  delete p;
+  return WAP_OK;
+}
+
+int wap_plan_set_config(wap_plan* p, int row_e, int col_e, int col_w) {
+  clear_error();
+  if (!p) return fail(WAP_ERR_ARG, "plan is NULL");
+  if (!config_valid(p, row_e, col_e, col_w))
+    return fail(WAP_ERR_ARG, "invalid launch configuration row_e=%d col_e=%d col_w=%d for %d x %d", row_e, col_e, col_w,
+                p->ny, p->nx);
+  p->row_e = row_e;
+  p->col_e = col_e;
+  p->col_w = col_w;
+  return upload_twiddles(p);
+}
+
+int wap_plan_get_config(const wap_plan* p, int* row_e, int* col_e, int* col_w) {
+  clear_error();
+  if (!p || !row_e || !col_e || !col_w) return fail(WAP_ERR_ARG, "NULL argument");
+  *row_e = p->row_e;
+  *col_e = p->col_e;
+  *col_w = p->col_w;
+  return WAP_OK;
+}
+
+int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double z, double energy, void* out,
+                          int out_c128, void* stream) {
+  clear_error();
+  if (!out) return fail(WAP_ERR_ARG, "out is NULL");
+  if (kind != WAP_TF_FRESNEL && kind != WAP_TF_ANGULAR) return fail(WAP_ERR_ARG, "unknown transfer function %d", kind);
+  if (n < 1 || m < 1) return fail(WAP_ERR_ARG, "bad shape %d x %d", n, m);
+  if (!(energy > 0) || !(ps0 > 0) || !(ps1 > 0)) return fail(WAP_ERR_ARG, "energy and sampling must be positive");
+  TfArgs a{kind, n, m, out_c128 ? 1 : 0, ps0, ps1, z, physics(energy, 1.0).lambda, out};
+  const long long total = (long long)n * m;
+  transfer_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
+  cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? WAP_OK : cuda_fail(err, "transfer_kernel");
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Fresnel / angular-spectrum forward
+// ----------------------------------------------------------------------------
+namespace wap {
+
+int check_common(const wap_plan* p, const float* V, int n_slices, int n_draws, const float* psi0, int n_probes,
+                 float* exit) {
+  if (!p) return fail(WAP_ERR_ARG, "plan is NULL");
+  if (!V || !psi0 || !exit) return fail(WAP_ERR_ARG, "V, psi0 and exit must be non-NULL device pointers");
+  if (n_slices < 1) return fail(WAP_ERR_ARG, "need at least one slice (got %d)", n_slices);
+  if (n_draws < 1) return fail(WAP_ERR_ARG, "n_draws must be >= 1");
+  if (n_probes < 1 || n_probes > p->max_batch)
+    return fail(WAP_ERR_ARG, "n_probes=%d outside [1, max_batch=%d]", n_probes, p->max_batch);
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != p->device) return fail(WAP_ERR_ARG, "plan was created on device %d, current device is %d", p->device, dev);
+  return WAP_OK;
+}
+
+RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw) {
+  RowArgs r{};
+  r.V = V;
+  r.draw = draw;
+  r.v_draw_stride = (long long)n_slices * p->ny * p->nx;
+  r.tw = p->tw_row;
+  r.ny = p->ny;
+  r.nx = p->nx;
+  r.scale = (float)(1.0 / ((double)p->ny * p->nx));
+  r.src_scale = 1.0f;
+  r.ri_a = (float)ph.ri_a;
+  r.ri_inv_den = (float)ph.ri_inv_den;
+  r.kphase = (float)ph.kphase;
+  r.e_plus_e0 = (float)ph.e_plus_e0;
+  return r;
+}
+
+ColArgs base_col_args(const wap_plan* p, const float* H) {
+  ColArgs c{};
+  c.H = reinterpret_cast<const float2*>(H);
+  c.tw = p->tw_col;
+  c.ny = p->ny;
+  c.nx = p->nx;
+  c.seed_scale = (float)((double)p->ny * p->nx);
+  return c;
+}
+
+// batch chunks of at most 65535 probes (grid.y limit)
+cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st) {
+  const int rows = rows_per_cta(p->nx, p->row_e, p->ny);
+  for (int b0 = 0; b0 < n_probes; b0 += 65535) {
+    r.probe0 = b0;
+    cudaError_t e = launch_row(p->nx, p->row_e, r, std::min(65535, n_probes - b0), rows, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t st) {
+  for (int b0 = 0; b0 < n_probes; b0 += 65535) {
+    c.probe0 = b0;
+    cudaError_t e = launch_col(p->ny, p->col_e, c, std::min(65535, n_probes - b0), p->col_w, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Forward multislice; snapshots of the wave entering slice s go to
+// snap + (s / snap_every) * plane when s % snap_every == 0 (snap_first = 0:
+// checkpoints), or the wave after every slice to stack (snap_first = 1).
+int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, const float* psi0,
+                    int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, double dz,
+                    double energy, float* exit, float* dp, float* stack, float* ckpt, int ckpt_every,
+                    cudaStream_t st) {
+  int rc = check_common(p, V, n_slices, n_draws, psi0, n_probes, exit);
+  if (rc) return rc;
+  if (!H) return fail(WAP_ERR_ARG, "H must be a non-NULL device pointer");
+  if (p->op != WAP_OP_FRESNEL_AS) return fail(WAP_ERR_ARG, "plan was not created for the Fresnel/AS path");
+  const Physics ph = physics(energy, dz);
+  const long long plane = (long long)p->ny * p->nx;
+  const int nck = ckpt ? (n_slices + ckpt_every - 1) / ckpt_every : 0;
+
+  RowArgs r = base_row_args(p, ph, V, n_slices, draw);
+  r.psi = reinterpret_cast<float2*>(exit);
+  r.psi_bstride = plane;
+  r.src = reinterpret_cast<const float2*>(psi0);
+  r.src_bstride = psi0_per_probe ? plane : 0;
+  r.shifts = positions;
+  ColArgs c = base_col_args(p, H);
+  c.psi = r.psi;
+  c.psi_bstride = plane;
+  c.dp = dp;
+
+  for (int s = 0; s <= n_slices; ++s) {
+    r.slice = s;
+    r.flags = (s == 0 ? ROW_LOAD_SRC : ROW_IFFT) | (s < n_slices ? (ROW_TRANS | ROW_FFT) : 0);
+    r.snap = nullptr;
+    if (stack && s >= 1) {
+      r.snap = reinterpret_cast<float2*>(stack) + (long long)(s - 1) * plane;
+      r.snap_bstride = (long long)n_slices * plane;
+    } else if (ckpt && s < n_slices && s % ckpt_every == 0) {
+      r.snap = reinterpret_cast<float2*>(ckpt) + (long long)(s / ckpt_every) * plane;
+      r.snap_bstride = (long long)nck * plane;
+    }
+    cudaError_t e = row_chunks(p, r, n_probes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "row pass");
+    if (s == n_slices) break;
+    c.flags = (s == n_slices - 1 && dp) ? COL_DP : 0;
+    e = col_chunks(p, c, n_probes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "column pass");
+  }
+  return WAP_OK;
+}
+
+}  // namespace wap
+
+extern "C" {
+
+int wap_multislice_fwd(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, const float* psi0,
+                       int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, double dz,
+                       double energy, float* exit, float* dp, float* stack, void* stream) {
+  clear_error();
+  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, dz, energy, exit,
+                         dp, stack, nullptr, 1, (cudaStream_t)stream);
+}
+
+int wap_multislice_fwd_ckpt(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw,
+                            const float* psi0, int n_probes, int psi0_per_probe, const int32_t* positions,
+                            const float* H, double dz, double energy, float* exit, float* dp, float* ckpt,
+                            int ckpt_every, void* stream) {
+  clear_error();
+  if (!ckpt) return fail(WAP_ERR_ARG, "ckpt must be a non-NULL device pointer");
+  if (ckpt_every < 1) return fail(WAP_ERR_ARG, "ckpt_every must be >= 1");
+  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, dz, energy, exit,
+                         dp, nullptr, ckpt, ckpt_every, (cudaStream_t)stream);
+}
+
+// ----------------------------------------------------------------------------
+// adjoint (gradient w.r.t. V)
+// ----------------------------------------------------------------------------
+int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, int n_probes,
+                       const float* H, double dz, double energy, const float* exit, const float* ckpt, int ckpt_every,
+                       const float* grad_dp, const float* grad_exit, float* grad_V, float* work, void* stream) {
+  clear_error();
+  int rc = check_common(p, V, n_slices, n_draws, exit, n_probes, const_cast<float*>(exit));
+  if (rc) return rc;
+  if (!H || !ckpt || !grad_V || !work) return fail(WAP_ERR_ARG, "H, ckpt, grad_V and work must be non-NULL");
+  if (!grad_dp && !grad_exit) return fail(WAP_ERR_ARG, "need grad_dp or grad_exit");
+  if (ckpt_every < 1) return fail(WAP_ERR_ARG, "ckpt_every must be >= 1");
+  if (p->op != WAP_OP_FRESNEL_AS) return fail(WAP_ERR_ARG, "plan was not created for the Fresnel/AS path");
+  cudaStream_t st = (cudaStream_t)stream;
+  const Physics ph = physics(energy, dz);
+  const long long plane = (long long)p->ny * p->nx;
+  const int k = ckpt_every;
+  const int nck = (n_slices + k - 1) / k;
+  const long long wstride = (long long)(k + 2) * plane;
+  float2* w = reinterpret_cast<float2*>(work);
+  float2* lam = w;                 // slot 0: adjoint state
+  float2* buf = w + plane;         // slot 1: recompute / seed buffer
+  float2* seg = w + 2 * plane;     // slots 2..k+1: psi_s of the segment
+  const float2* ck = reinterpret_cast<const float2*>(ckpt);
+  cudaError_t e;
+
+  // seed: lambda_psi_N = grad_exit / 2 + F^H (g Z), Z = fft2(exit);
+  // lambda_a_{N-1} = ifft2(conj(H) fft2(lambda_psi_N))
+  RowArgs r = base_row_args(p, ph, V, n_slices, draw);
+  r.psi = lam;
+  r.psi_bstride = wstride;
+  r.src = reinterpret_cast<const float2*>(exit);
+  r.src_bstride = plane;
+  r.flags = ROW_LOAD_SRC | ROW_FFT;
+  if ((e = row_chunks(p, r, n_probes, st)) != cudaSuccess) return cuda_fail(e, "seed row pass");
+  if (grad_exit) {
+    r.psi = buf;
+    r.src = reinterpret_cast<const float2*>(grad_exit);
+    r.flags = ROW_LOAD_SRC | ROW_FFT | ROW_SCALE_SRC;
+    r.src_scale = 0.5f;
+    if ((e = row_chunks(p, r, n_probes, st)) != cudaSuccess) return cuda_fail(e, "seed row pass");
+    r.src_scale = 1.0f;
+  }
+  ColArgs c = base_col_args(p, H);
+  c.psi = lam;
+  c.psi_bstride = wstride;
+  c.flags = COL_SEED | COL_CONJ_H;
+  c.g = grad_dp;
+  c.seed2 = grad_exit ? buf : nullptr;
+  c.seed2_bstride = wstride;
+  if ((e = col_chunks(p, c, n_probes, st)) != cudaSuccess) return cuda_fail(e, "seed column pass");
+
+  for (int j = nck - 1; j >= 0; --j) {
+    const int s0 = j * k, s1 = std::min(s0 + k, n_slices);
+    // recompute psi_{s0+1} .. psi_{s1-1} from the checkpoint psi_{s0}
+    for (int s = s0; s < s1 - 1; ++s) {
+      RowArgs q = base_row_args(p, ph, V, n_slices, draw);
+      q.psi = buf;
+      q.psi_bstride = wstride;
+      q.slice = s;
+      if (s == s0) {
+        q.src = ck + (long long)j * plane;
+        q.src_bstride = (long long)nck * plane;
+        q.flags = ROW_LOAD_SRC | ROW_TRANS | ROW_FFT;
+      } else {
+        q.flags = ROW_IFFT | ROW_TRANS | ROW_FFT;
+        q.snap = seg + (long long)(s - s0) * plane;
+        q.snap_bstride = wstride;
+      }
+      if ((e = row_chunks(p, q, n_probes, st)) != cudaSuccess) return cuda_fail(e, "recompute row pass");
+      ColArgs cc = base_col_args(p, H);
+      cc.psi = buf;
+      cc.psi_bstride = wstride;
+      if ((e = col_chunks(p, cc, n_probes, st)) != cudaSuccess) return cuda_fail(e, "recompute column pass");
+    }
+    if (s1 - 1 > s0) {
+      RowArgs q = base_row_args(p, ph, V, n_slices, draw);
+      q.psi = buf;
+      q.psi_bstride = wstride;
+      q.slice = s1 - 1;
+      q.flags = ROW_IFFT;
+      q.snap = seg + (long long)(s1 - 1 - s0) * plane;
+      q.snap_bstride = wstride;
+      if ((e = row_chunks(p, q, n_probes, st)) != cudaSuccess) return cuda_fail(e, "recompute row pass");
+    }
+    // adjoint sweep s1-1 .. s0
+    for (int s = s1 - 1; s >= s0; --s) {
+      RowArgs a = base_row_args(p, ph, V, n_slices, draw);
+      a.psi = lam;
+      a.psi_bstride = wstride;
+      a.slice = s;
+      a.flags = ROW_IFFT | ROW_ADJOINT | (s > 0 ? ROW_FFT : 0);
+      if (s == s0) {
+        a.aux = ck + (long long)j * plane;
+        a.aux_bstride = (long long)nck * plane;
+      } else {
+        a.aux = seg + (long long)(s - s0) * plane;
+        a.aux_bstride = wstride;
+      }
+      a.grad = grad_V;
+      if ((e = row_chunks(p, a, n_probes, st)) != cudaSuccess) return cuda_fail(e, "adjoint row pass");
+      if (s == 0) break;
+      ColArgs ca = base_col_args(p, H);
+      ca.psi = lam;
+      ca.psi_bstride = wstride;
+      ca.flags = COL_CONJ_H;
+      if ((e = col_chunks(p, ca, n_probes, st)) != cudaSuccess) return cuda_fail(e, "adjoint column pass");
+    }
+  }
+  return WAP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,297 @@
+// In-house complex64 FFT core for the multislice passes (sm_100a).
+//
+// One N-point transform is computed by T = N/E threads; thread t holds the E
+// elements x[t + T*e] (e = 0..E-1) in registers.  The transform is a radix-E
+// Stockham autosort (plus one smaller remainder radix), numpy.fft sign and
+// normalisation conventions: forward exp(-2 pi i jk/N) unnormalised, inverse
+// exp(+2 pi i jk/N) unnormalised (callers apply 1/N).
+//
+// Stage s (radix R, span L = product of earlier radices), butterfly
+// b = t + T*q, k = b mod L:
+//   inputs  x[b + (N/R) j] = register slot q + (E/R) j
+//   twiddle W_{LR}^{jk}, from a per-stage table laid out [j][k] so that
+//           consecutive threads read consecutive words
+//   outputs y_m -> position (b - k) R + k + m L, exchanged through shared
+//           memory for every stage but the last.
+// After the last stage thread t again holds X[t + T*e] in slot e, so a forward
+// transform, a pointwise multiply and an inverse transform chain in registers.
+// The in-register radix-2/4/8/16 butterflies use split-radix-free 4x4 / 2x4
+// decompositions with exact constants of the 16th roots of unity.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace wap {
+
+// ----------------------------------------------------------------------------
+// plan arithmetic, shared by host (twiddle tables) and device (stages)
+// ----------------------------------------------------------------------------
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
+
+template <int N, int E>
+struct FFTPlan {
+  static_assert((N & (N - 1)) == 0 && (E & (E - 1)) == 0, "powers of two");
+  static_assert(E >= 2 && E <= 16 && N >= E, "2 <= E <= 16 <= N");
+  static constexpr int T = N / E;
+  static constexpr int LOGN = ilog2c(N);
+  static constexpr int LOGE = ilog2c(E);
+  static constexpr int NFULL = LOGN / LOGE;
+  static constexpr int REM = 1 << (LOGN % LOGE);
+  static constexpr int S = NFULL + (REM > 1 ? 1 : 0);
+  __host__ __device__ static constexpr int radix(int s) { return s < NFULL ? E : REM; }
+  __host__ __device__ static constexpr int span(int s) {
+    int L = 1;
+    for (int i = 0; i < s; ++i) L *= radix(i);
+    return L;
+  }
+  // offset of stage s in the concatenated twiddle table (stages s >= 1)
+  __host__ __device__ static constexpr int tw_offset(int s) {
+    int off = 0;
+    for (int i = 1; i < s; ++i) off += radix(i) * span(i);
+    return off;
+  }
+  static constexpr int TW_SIZE = tw_offset(S) > 0 ? tw_offset(S) : 1;
+};
+
+// Runtime mirror of FFTPlan for the host-side table builder.
+struct PlanShape {
+  int n, e, nfull, rem, stages;
+  __host__ __device__ int radix(int s) const { return s < nfull ? e : rem; }
+  __host__ __device__ int span(int s) const {
+    int L = 1;
+    for (int i = 0; i < s; ++i) L *= radix(i);
+    return L;
+  }
+  __host__ __device__ int tw_offset(int s) const {
+    int off = 0;
+    for (int i = 1; i < s; ++i) off += radix(i) * span(i);
+    return off;
+  }
+  __host__ __device__ int tw_size() const { int t = tw_offset(stages); return t > 0 ? t : 1; }
+};
+
+__host__ __device__ inline PlanShape make_plan_shape(int n, int e) {
+  PlanShape p{};
+  int logn = ilog2c(n), loge = ilog2c(e);
+  p.n = n;
+  p.e = e;
+  p.nfull = logn / loge;
+  p.rem = 1 << (logn % loge);
+  p.stages = p.nfull + (p.rem > 1 ? 1 : 0);
+  return p;
+}
+
+// ----------------------------------------------------------------------------
+// complex helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// multiply by -i (forward sign) or +i (inverse sign)
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// cos / sin of 2 pi m / 16, exact to float rounding
+__device__ __forceinline__ float cos16(int m) {
+  switch (m & 15) {
+    case 0: return 1.0f;
+    case 1: return 0.92387953251128674f;
+    case 2: return 0.70710678118654752f;
+    case 3: return 0.38268343236508977f;
+    case 4: return 0.0f;
+    case 5: return -0.38268343236508977f;
+    case 6: return -0.70710678118654752f;
+    case 7: return -0.92387953251128674f;
+    case 8: return -1.0f;
+    case 9: return -0.92387953251128674f;
+    case 10: return -0.70710678118654752f;
+    case 11: return -0.38268343236508977f;
+    case 12: return 0.0f;
+    case 13: return 0.38268343236508977f;
+    case 14: return 0.70710678118654752f;
+    default: return 0.92387953251128674f;
+  }
+}
+__device__ __forceinline__ float sin16(int m) { return cos16(m - 4); }
+
+// a * W16^m with W16 = exp(-+2 pi i / 16); m is a compile-time constant after
+// unrolling, so the branches fold away.
+template <bool INV>
+__device__ __forceinline__ float2 tw16(float2 a, int m) {
+  m &= 15;
+  if (m == 0) return a;
+  if (m == 8) return make_float2(-a.x, -a.y);
+  if (m == 4) return mul_mi<INV>(a);
+  if (m == 12) return mul_mi<!INV>(a);
+  const float c = cos16(m);
+  const float s = INV ? sin16(m) : -sin16(m);  // twiddle = c + i s
+  if ((m & 3) == 2) {
+    // |c| == |s|: two adds, two multiplies
+    if (c == s) return make_float2(c * (a.x - a.y), c * (a.y + a.x));
+    return make_float2(c * (a.x + a.y), c * (a.y - a.x));
+  }
+  return make_float2(fmaf(c, a.x, -s * a.y), fmaf(c, a.y, s * a.x));
+}
+
+// ----------------------------------------------------------------------------
+// in-register DFT codelets, natural order in and out
+// ----------------------------------------------------------------------------
+template <bool INV>
+__device__ __forceinline__ void dft2(float2& a0, float2& a1) {
+  float2 t = a0;
+  a0 = cadd(t, a1);
+  a1 = csub(t, a1);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
+  float2 t2 = cadd(a1, a3), t3 = mul_mi<INV>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&a)[R]) {
+  if constexpr (R == 1) {
+  } else if constexpr (R == 2) {
+    dft2<INV>(a[0], a[1]);
+  } else if constexpr (R == 4) {
+    dft4<INV>(a[0], a[1], a[2], a[3]);
+  } else if constexpr (R == 8) {
+    // n = n1 + 2 n2, k = 4 k1 + k2
+#pragma unroll
+    for (int n1 = 0; n1 < 2; ++n1) dft4<INV>(a[n1], a[n1 + 2], a[n1 + 4], a[n1 + 6]);
+    // Y[n1][k2] sits in a[n1 + 2 k2]
+#pragma unroll
+    for (int k2 = 1; k2 < 4; ++k2) a[1 + 2 * k2] = tw16<INV>(a[1 + 2 * k2], 2 * k2);
+    float2 o[8];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+      float2 y0 = a[2 * k2], y1 = a[1 + 2 * k2];
+      o[k2] = cadd(y0, y1);
+      o[4 + k2] = csub(y0, y1);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = o[i];
+  } else if constexpr (R == 16) {
+    // n = n1 + 4 n2, k = 4 k1 + k2
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) dft4<INV>(a[n1], a[n1 + 4], a[n1 + 8], a[n1 + 12]);
+    // Y[n1][k2] sits in a[n1 + 4 k2]
+#pragma unroll
+    for (int n1 = 1; n1 < 4; ++n1)
+#pragma unroll
+      for (int k2 = 1; k2 < 4; ++k2) a[n1 + 4 * k2] = tw16<INV>(a[n1 + 4 * k2], n1 * k2);
+    float2 o[16];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+      float2 y0 = a[4 * k2], y1 = a[1 + 4 * k2], y2 = a[2 + 4 * k2], y3 = a[3 + 4 * k2];
+      dft4<INV>(y0, y1, y2, y3);
+      o[k2] = y0;
+      o[4 + k2] = y1;
+      o[8 + k2] = y2;
+      o[12 + k2] = y3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = o[i];
+  } else {
+    static_assert(R <= 16, "radix");
+  }
+}
+
+// ----------------------------------------------------------------------------
+// shared-memory exchange policies
+// ----------------------------------------------------------------------------
+// One transform per row segment of shared memory; index p padded by one word
+// per 16 so that radix-R Stockham scatters are bank-conflict free.
+template <bool WARP_LOCAL>
+struct RowExchange {
+  float2* base;
+  __device__ __forceinline__ void st(int p, float2 v) const { base[p + (p >> 4)] = v; }
+  __device__ __forceinline__ float2 ld(int p) const { return base[p + (p >> 4)]; }
+  __device__ __forceinline__ void sync() const {
+    if constexpr (WARP_LOCAL) __syncwarp();
+    else __syncthreads();
+  }
+  __host__ __device__ static constexpr int padded(int n) { return n + (n >> 4); }
+};
+
+// One transform per column of a row-major [N][W] tile (lanes run along the
+// columns, so stores of one Stockham position by a warp are contiguous).
+struct ColExchange {
+  float2* base;
+  int w, c;
+  __device__ __forceinline__ void st(int p, float2 v) const { base[p * w + c] = v; }
+  __device__ __forceinline__ float2 ld(int p) const { return base[p * w + c]; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// ----------------------------------------------------------------------------
+// Stockham stages
+// ----------------------------------------------------------------------------
+template <int N, int E, int SI, bool INV, class X>
+__device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, const float2* __restrict__ tw) {
+  using P = FFTPlan<N, E>;
+  constexpr int R = P::radix(SI);
+  constexpr int L = P::span(SI);
+  constexpr int B = E / R;
+  constexpr int T = P::T;
+  constexpr bool LAST = (SI == P::S - 1);
+  constexpr int OFF = P::tw_offset(SI);
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const int b = t + T * q;
+    const int k = b & (L - 1);
+    float2 a[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) a[j] = v[q + B * j];
+    if constexpr (L > 1) {
+#pragma unroll
+      for (int j = 1; j < R; ++j) {
+        const float2 w = tw[OFF + j * L + k];
+        a[j] = INV ? cmulc(a[j], w) : cmul(a[j], w);
+      }
+    }
+    dft<R, INV>(a);
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[q + B * m] = a[m];
+  }
+  if constexpr (!LAST) {
+    xs.sync();  // every thread has finished reading the previous contents
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int b = t + T * q;
+      const int k = b & (L - 1);
+      const int base = (b - k) * R + k;
+#pragma unroll
+      for (int m = 0; m < R; ++m) xs.st(base + m * L, v[q + B * m]);
+    }
+    xs.sync();
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
+  }
+}
+
+template <int N, int E, bool INV, class X, int SI = 0>
+__device__ __forceinline__ void fft(float2 (&v)[E], int t, const X& xs, const float2* __restrict__ tw) {
+  if constexpr (SI < FFTPlan<N, E>::S) {
+    fft_stage<N, E, SI, INV>(v, t, xs, tw);
+    fft<N, E, INV, X, SI + 1>(v, t, xs, tw);
+  }
+}
+
+}  // namespace wap

@@ -1,0 +1,57 @@
+// Internal declarations shared by the libwap.so translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/wap.h"
+
+struct wap_plan {
+  int device = 0;
+  int ny = 0, nx = 0, max_batch = 0, op = 0, n_bins = 0;
+  int row_e = 16, col_e = 16, col_w = 16;   // FFT launch shape (autotuned)
+  float2* tw_row = nullptr;                 // twiddles for nx / row_e
+  float2* tw_col = nullptr;                 // twiddles for ny / col_e
+  // WPM workspace
+  float2* fields = nullptr;                 // (max_batch, n_bins, ny, nx)
+  float2* dpbuf = nullptr;                  // (max_batch, ny, nx)
+  float2* hvac = nullptr;                   // (ny, nx)
+  float* ky2 = nullptr;
+  float* kx2 = nullptr;
+  double hvac_key[4] = {0, 0, 0, 0};        // (dy, dx, dz, energy) of hvac
+  float* refs = nullptr;                    // (draws, n_slices, n_bins)
+  size_t refs_cap = 0;
+};
+
+namespace wap {
+
+struct Physics {
+  double e0, lambda, ri_a, ri_inv_den, kphase, k0, e_plus_e0;
+};
+
+Physics physics(double energy, double dz);
+std::vector<float2> twiddle_table(int n, int e);
+
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+void clear_error();
+const char* last_error();
+
+int check_common(const wap_plan* p, const float* V, int n_slices, int n_draws, const float* psi0, int n_probes,
+                 float* exit);
+int rows_per_cta(int nx, int e, int ny);
+bool size_supported(int n);
+
+struct RowArgs;
+struct ColArgs;
+struct WpmColArgs;
+struct WpmRowArgs;
+cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream_t st);
+cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st);
+cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cudaStream_t st);
+cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st);
+cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
+RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
+
+}  // namespace wap
