@@ -1,0 +1,419 @@
+"""Benchmark: batched uneven 4D-STEM multislice scan on B200.
+
+Workload (one "step"): 1024 probes on 256x256 windows (16x16 raster x 4
+frozen-phonon draws, 80 slices) plus 64 probes on 512x512 windows (8x8
+raster, 150 slices), diamond [100] lattice, 300 keV, angular-spectrum
+propagator, 25 mrad / -50 A probes, complex64 waves, float32 diffraction
+patterns - 91 520 slice-steps per step.
+
+Printed JSON line (rank 0):
+  value       slice-steps/s of the batched path, inputs resident in HBM
+  e2e         the same through the public API (simulate_fresnel_as with
+              positions/draws) from pinned host buffers, host<->device copies
+              of the potential and of the diffraction patterns inside the
+              timed region
+  plain       slice-steps/s of the one-probe-per-launch path (same kernels)
+  grad_over_fwd  t(forward + adjoint gradient) / t(forward) on the
+              512^2, 64-slice, 64-probe inverse problem (checkpoint every 8)
+  err_vs_fp64 rel-L2 of exit wave and diffraction pattern vs the FP64 oracle
+  roofline    dominant pass kernel: algorithmic bytes / device time vs the
+              measured HBM copy bandwidth
+  cpu_baseline  the NumPy/SciPy FP64 restatement on the host cores
+
+``--impl reference`` times that CPU restatement alone as the reference arm.
+Multi-GPU (torchrun): every rank runs its own copy of the scan (probes shard
+with no data-path collective): weak scaling, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "slice-steps/s at 1 B200 batched vs plain; grad/fwd cost; err vs FP64"
+WORKLOAD = ("batched uneven 4D-STEM scan: 1024 probes 256^2 x 80 slices (16x16 raster x 4 phonon draws) "
+            "+ 64 probes 512^2 x 150 slices (8x8 raster); diamond [100], 300 keV, angular spectrum")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="wap", choices=["wap", "reference"])
+    ap.add_argument("--small", action="store_true", help="tiny workload (testing the harness)")
+    ap.add_argument("--no-extras", action="store_true", help="skip plain/grad/err/cpu sections")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def mix_rate(t_per_step_by_class, counts):
+    """slice-steps/s of the workload mix given seconds per slice-step per class."""
+    total = sum(counts)
+    return total / sum(t * n for t, n in zip(t_per_step_by_class, counts))
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_reference_sample(classes_host, scale=1, mode="fp64"):
+    """Time the oracle restatement on a bounded sample of each grid class
+    (16*scale probes of the 256^2 class, 2*scale of the 512^2 class, 8 slices).
+
+    Returns (slice-steps/s for the workload mix, cores, sample description)."""
+    from oracle import propagation_oracle as O
+    cores = os.cpu_count() or 1
+    O.set_workers(cores)
+    per_step = []
+    desc = []
+    for w in classes_host:
+        H = O.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+        nb = (16 if w.ny <= 256 else 2) * scale
+        ns = 8
+        probes = np.stack([O.move_probe(w.probe, tuple(p)) for p in w.positions[:nb]])
+        t0 = time.perf_counter()
+        O.simulate_fresnel_as(w.potential[0, :ns], probes, H, w.dz, w.energy, mode=mode, return_wavefronts=False)
+        dt = time.perf_counter() - t0
+        per_step.append(dt / (nb * ns))
+        desc.append(f"{nb} probes x {ns} slices at {w.ny}^2")
+    rate = mix_rate(per_step, [w.n_probes * w.n_slices for w in classes_host])
+    return rate, cores, "; ".join(desc) + f" (oracle {mode}, scipy.fft workers={cores}), scaled to the workload mix"
+
+
+def run_reference(args, classes_host, rank):
+    if rank != 0:
+        return
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, cores, desc = cpu_reference_sample(classes_host)
+        if i >= args.warmup:
+            rates.append(r)
+    v = statistics.median(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "slice-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(c.n_probes * c.n_slices for c in classes_host) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "config": {"workload": WORKLOAD},
+            "cpu_baseline": {"value": v, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "slice-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index=0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.strip().split(", ") for l in open(self.f.name) if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import wideanglepropagation_b200.synthetic as S
+    classes_host = S.batched_scan(0, small=args.small)
+
+    if args.impl == "reference":
+        run_reference(args, classes_host, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from wideanglepropagation_b200 import _lib
+    import wideanglepropagation_b200 as wap
+    from wideanglepropagation_b200.scan import BatchedScan, to_device_class
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    _lib.lib()
+    launches0 = _lib.launch_count()
+    classes = [to_device_class(w, dev) for w in classes_host]
+    scan = BatchedScan(classes, mode="batched")
+    total_ss = scan.slice_steps()
+
+    # --- headline: batched, inputs resident in HBM --------------------------
+    for _ in range(args.warmup):
+        scan.step()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = _lib.launch_count()
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(args.steps):
+        scan.step()
+    stop.record()
+    torch.cuda.synchronize()
+    l1 = _lib.launch_count()
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(start.elapsed_time(stop))
+    ms_per_step = ms / args.steps
+    value = total_ss * world / (ms_per_step / 1e3)
+    gpu_launches = l1 - l0
+
+    extras = {}
+    # --- roofline: per-pass device time with the library's event tracing -----
+    _lib.profile_reset()
+    _lib.profile_enable(True)
+    for _ in range(max(1, min(args.steps, 3))):
+        scan.step()
+    torch.cuda.synchronize()
+    _lib.profile_enable(False)
+    kinds = {}
+    for k, name in _lib.KIND_NAMES.items():
+        n, kms, by = _lib.profile_read(k)
+        if n:
+            kinds[name] = (n, kms, by)
+    _lib.profile_reset()
+    dom = max(kinds, key=lambda k: kinds[k][1])
+    n, kms, by = kinds[dom]
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = by / (kms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": _ncu_traffic(dom), "kernel": dom, "peak_source": peak_src,
+                "launches": n, "avg_launch_us": 1e3 * kms / n,
+                "share": {k: v[1] / sum(x[1] for x in kinds.values()) for k, v in kinds.items()}}
+
+    if not args.no_extras and rank == 0:
+        extras.update(_plain(classes, args))
+        extras.update(_grad_ratio(args))
+        extras.update(_err_vs_fp64(classes, classes_host))
+
+    # --- e2e through the public API from pinned host buffers ------------------
+    e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
+
+    cpu = None
+    if rank == 0 and not args.no_extras:
+        r, cores, desc = cpu_reference_sample(classes_host, scale=4, mode="fp64")
+        cpu = {"value": r, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "slice-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "slice_steps_per_step": total_ss,
+                           "pixel_slice_steps_per_step": sum(c.pixel_slice_steps for c in classes),
+                           "l2": "inputs larger than L2 (potential 241 MB, waves 640 MB per step)",
+                           "mode": "batched per-pass launches", "parallelism": f"probe shards x{world}"},
+                "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clk,
+                "cpu_baseline": cpu}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _ncu_traffic(kernel):
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def _plain(classes, args):
+    import torch
+    from wideanglepropagation_b200.scan import BatchedScan
+    # one probe per launch sequence on a subset of each class (timing scales per slice-step)
+    plain = BatchedScan(classes, mode="plain", plain_subset=16)
+    plain.step()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per = []
+    for c in classes:
+        sub = BatchedScan([c], mode="plain", plain_subset=16)
+        s.record()
+        sub.step()
+        e.record()
+        torch.cuda.synchronize()
+        per.append(s.elapsed_time(e) / 1e3 / sub.slice_steps())
+    rate = mix_rate(per, [c.slice_steps for c in classes])
+    # batched per class for the same comparison
+    bper = []
+    for c in classes:
+        sub = BatchedScan([c], mode="batched")
+        sub.step()
+        s.record()
+        sub.step()
+        e.record()
+        torch.cuda.synchronize()
+        bper.append(s.elapsed_time(e) / 1e3 / sub.slice_steps())
+    return {"plain": {"value": rate, "unit": "slice-steps/s", "sample": "16 probes per class, one probe per launch"},
+            "per_class_slice_steps_per_s": {f"{c.ny}x{c.nx}": {"batched": 1 / b, "plain": 1 / p}
+                                            for c, b, p in zip(classes, bper, per)}}
+
+
+def _grad_ratio(args):
+    import torch
+    import wideanglepropagation_b200 as wap
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    w = wap.synthetic.inverse_problem(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy, dtype=torch.complex64)
+    probe = torch.as_tensor(w.probe).to(dev)
+    pos = torch.as_tensor(w.positions).to(dev)
+    Vt = torch.as_tensor(w.potential[0]).to(dev)
+    _, target = wap.simulate_fresnel_as(Vt, probe, H, w.dz, w.energy, positions=pos, return_wavefronts=False)
+    V = torch.zeros_like(Vt, requires_grad=True)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def fwd():
+        with torch.no_grad():
+            return wap.simulate_fresnel_as(V, probe, H, w.dz, w.energy, positions=pos, return_wavefronts=False)
+
+    def step(k):
+        V.grad = None
+        _, dp = simulate_fresnel_as_differentiable(V, probe, H, w.dz, w.energy, positions=pos, ckpt_every=k)
+        ((dp - target) ** 2).sum().backward()
+
+    out = {}
+    for _ in range(2):
+        fwd(); step(8); step(1)
+    torch.cuda.synchronize()
+    reps = 3
+    s.record()
+    for _ in range(reps):
+        fwd()
+    e.record()
+    torch.cuda.synchronize()
+    t_f = s.elapsed_time(e) / reps
+    for k in (8, 1):
+        s.record()
+        for _ in range(reps):
+            step(k)
+        e.record()
+        torch.cuda.synchronize()
+        out[k] = s.elapsed_time(e) / reps / t_f
+    return {"grad_over_fwd": out[8], "grad_over_fwd_ckpt1": out[1], "grad_fwd_ms": t_f,
+            "grad_workload": "512^2, 64 slices x 2 A, 300 keV, 64 probes (8x8), L = sum(|FFT psi|^2 - I)^2"}
+
+
+def _err_vs_fp64(classes, classes_host):
+    import torch
+    import wideanglepropagation_b200 as wap
+    from oracle import propagation_oracle as O
+    errs = {}
+    for c, w in zip(classes, classes_host):
+        b = 0
+        H = O.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+        p0 = O.move_probe(w.probe, tuple(w.positions[b]))
+        rex, rdp, _ = O.simulate_fresnel_as(w.potential[w.draw_of_probe[b]], p0, H, w.dz, w.energy,
+                                            return_wavefronts=False)
+        torch.cuda.synchronize()
+        errs[f"{w.ny}x{w.nx}"] = {"exit": O.rel_l2(c.exit[b].cpu().numpy(), rex),
+                                  "dp": O.rel_l2(c.dp[b].cpu().numpy(), rdp)}
+    return {"err_vs_fp64": errs}
+
+
+def _e2e(classes_host, args, dev, barrier, max_over_ranks, world):
+    import torch
+    import wideanglepropagation_b200 as wap
+    host = []
+    for w in classes_host:
+        V = torch.from_numpy(w.potential).pin_memory()
+        H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy,
+                                                    dtype=torch.complex64)
+        host.append((w, V, torch.from_numpy(w.probe).pin_memory(), torch.from_numpy(w.positions).pin_memory(),
+                     torch.from_numpy(w.draw_of_probe).pin_memory(), H,
+                     torch.empty((w.n_probes, w.ny, w.nx), dtype=torch.float32).pin_memory()))
+    h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
+    d2h = sum(o.numel() * 4 for *_, o in host)
+
+    def step():
+        for w, V, p, q, d, H, out in host:
+            _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False)
+            out.copy_(dp, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.steps):
+        step()
+    e.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(s.elapsed_time(e)) / args.steps
+    total = sum(w.n_probes * w.n_slices for w in classes_host)
+    return {"value": total * world / (ms / 1e3), "unit": "slice-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "simulate_fresnel_as(positions=, draw=)"}
+
+
+if __name__ == "__main__":
+    main()

@@ -119,6 +119,23 @@ int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws
                        const float* grad_dp, const float* grad_exit, float* grad_V,
                        float* work, void* stream);
 
+/* Kernel-level tracing (no counterpart in the reference, which has none).
+ * While enabled, each pass launch is bracketed by CUDA events on its stream
+ * and tagged with its kind and algorithmic bytes (wave in/out, potential,
+ * snapshots).  wap_profile_read waits for the recorded events and returns the
+ * launch count, summed device milliseconds and summed bytes of one kind. */
+#define WAP_KIND_ROW 0        /* row pass (transmission + row FFTs) */
+#define WAP_KIND_COL 1        /* column pass (column FFTs + propagator) */
+#define WAP_KIND_WPM_COL 2    /* WPM column pass (K reference fields) */
+#define WAP_KIND_WPM_ROW 3    /* WPM row pass (K row IFFTs + blend) */
+#define WAP_KIND_WPM_BINS 4   /* WPM per-slice bin edges */
+#define WAP_KIND_SCHED 5      /* persistent batched scheduler */
+/* Number of kernels this library has launched in this process (all kinds). */
+long long wap_launch_count(void);
+int wap_profile_enable(int on);
+int wap_profile_reset(void);
+int wap_profile_read(int kind, long long* launches, double* total_ms, double* total_bytes);
+
 #ifdef __cplusplus
 }
 #endif

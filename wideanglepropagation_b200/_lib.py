@@ -41,7 +41,15 @@ SIGNATURES = {
     "wap_wpm_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P]),
     "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
     "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "wap_launch_count": (ctypes.c_longlong, []),
+    "wap_profile_enable": (_I, [_I]),
+    "wap_profile_reset": (_I, []),
+    "wap_profile_read": (_I, [_I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
 }
+
+KIND_ROW, KIND_COL, KIND_WPM_COL, KIND_WPM_ROW, KIND_WPM_BINS, KIND_SCHED = range(6)
+KIND_NAMES = {KIND_ROW: "row_pass_kernel", KIND_COL: "col_pass_kernel", KIND_WPM_COL: "wpm_col_kernel",
+              KIND_WPM_ROW: "wpm_row_kernel", KIND_WPM_BINS: "wpm_bins_kernel", KIND_SCHED: "scan_persistent_kernel"}
 
 _lib = None
 _lock = threading.Lock()
@@ -84,3 +92,23 @@ def check(rc: int) -> None:
 
 def version() -> str:
     return lib().wap_version().decode()
+
+
+def profile_enable(on: bool) -> None:
+    check(lib().wap_profile_enable(1 if on else 0))
+
+
+def profile_reset() -> None:
+    check(lib().wap_profile_reset())
+
+
+def profile_read(kind: int):
+    """(launches, device ms, algorithmic bytes) recorded for one pass kind."""
+    n, ms, by = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+    check(lib().wap_profile_read(kind, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
+    return n.value, ms.value, by.value
+
+
+def launch_count() -> int:
+    """Kernels launched by libwap.so in this process so far."""
+    return int(lib().wap_launch_count())

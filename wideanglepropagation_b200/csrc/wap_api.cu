@@ -97,6 +97,7 @@ static cudaError_t launch_row_t(const RowArgs& a, int nb, int rows, cudaStream_t
   const size_t smem = row_smem_bytes<N, E>(rows, 0);
   cudaError_t err = prep_smem(row_pass_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
+  count_launch();
   row_pass_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -106,6 +107,7 @@ static cudaError_t launch_col_t(const ColArgs& a, int nb, int w, cudaStream_t st
   const size_t smem = col_smem_bytes<N, E>(w, 0);
   cudaError_t err = prep_smem(col_pass_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
+  count_launch();
   col_pass_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -115,6 +117,7 @@ static cudaError_t launch_wpm_col_t(const WpmColArgs& a, int nb, int w, cudaStre
   const size_t smem = col_smem_bytes<N, E>(w, a.K * (int)sizeof(float));
   cudaError_t err = prep_smem(wpm_col_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
+  count_launch();
   wpm_col_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -125,6 +128,7 @@ static cudaError_t launch_wpm_row_t(const WpmRowArgs& a, int nb, int rows, cudaS
   const size_t smem = row_smem_bytes<N, E>(rows, extra);
   cudaError_t err = prep_smem(wpm_row_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
+  count_launch();
   wpm_row_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -333,6 +337,7 @@ int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double
   if (!(energy > 0) || !(ps0 > 0) || !(ps1 > 0)) return fail(WAP_ERR_ARG, "energy and sampling must be positive");
   TfArgs a{kind, n, m, out_c128 ? 1 : 0, ps0, ps1, z, physics(energy, 1.0).lambda, out};
   const long long total = (long long)n * m;
+  count_launch();
   transfer_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
   cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? WAP_OK : cuda_fail(err, "transfer_kernel");
@@ -386,23 +391,45 @@ ColArgs base_col_args(const wap_plan* p, const float* H) {
   return c;
 }
 
+// algorithmic bytes of one pass over n_probes waves (per pixel: wave in 8,
+// wave out 8, potential 4, snapshot 8, forward wave 8, gradient RMW 8; the
+// transfer function is counted once per launch)
+static double row_bytes(const wap_plan* p, const RowArgs& r, int n_probes) {
+  double per = 16;
+  if (r.flags & (ROW_TRANS | ROW_ADJOINT)) per += 4;
+  if (r.snap) per += 8;
+  if (r.flags & ROW_ADJOINT) per += 16;
+  return per * (double)p->ny * p->nx * n_probes;
+}
+
+static double col_bytes(const wap_plan* p, const ColArgs& c, int n_probes) {
+  double per = 16;
+  if (c.flags & COL_DP) per += 4;
+  if (c.flags & COL_SEED) per += 4 + (c.seed2 ? 8 : 0);
+  return per * (double)p->ny * p->nx * n_probes + ((c.flags & COL_NO_H) ? 0.0 : 8.0 * p->ny * p->nx);
+}
+
 // batch chunks of at most 65535 probes (grid.y limit)
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st) {
   const int rows = rows_per_cta(p->nx, p->row_e, p->ny);
+  const ProfToken tok = prof_begin(WAP_KIND_ROW, st);
   for (int b0 = 0; b0 < n_probes; b0 += 65535) {
     r.probe0 = b0;
     cudaError_t e = launch_row(p->nx, p->row_e, r, std::min(65535, n_probes - b0), rows, st);
     if (e != cudaSuccess) return e;
   }
+  prof_end(tok, st, row_bytes(p, r, n_probes));
   return cudaSuccess;
 }
 
 cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t st) {
+  const ProfToken tok = prof_begin(WAP_KIND_COL, st);
   for (int b0 = 0; b0 < n_probes; b0 += 65535) {
     c.probe0 = b0;
     cudaError_t e = launch_col(p->ny, p->col_e, c, std::min(65535, n_probes - b0), p->col_w, st);
     if (e != cudaSuccess) return e;
   }
+  prof_end(tok, st, col_bytes(p, c, n_probes));
   return cudaSuccess;
 }
 

@@ -54,4 +54,14 @@ cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cud
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
 RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
 
+// kernel-level tracing (wap_prof.cu)
+struct ProfToken {
+  bool active;
+  int kind;
+  cudaEvent_t a, b;
+};
+ProfToken prof_begin(int kind, cudaStream_t st);
+void count_launch();  // every kernel launch of the library bumps wap_launch_count()
+void prof_end(const ProfToken& t, cudaStream_t st, double bytes);
+
 }  // namespace wap

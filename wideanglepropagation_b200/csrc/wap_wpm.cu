@@ -78,14 +78,20 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
   const double key[4] = {sampling_y, sampling_x, dz, energy};
   if (!std::equal(key, key + 4, p->hvac_key)) {
     HvacArgs h{p->ny, p->nx, sampling_y, sampling_x, dz, ph.k0, p->hvac, p->ky2, p->kx2};
+    count_launch();
     wpm_vacuum_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(h);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "wpm_vacuum_kernel");
     std::copy(key, key + 4, p->hvac_key);
   }
 
   WpmBinsArgs bargs{V, p->refs, (int)plane, n_slices, K, (float)ph.ri_a, (float)ph.ri_inv_den, power_spacing};
-  wpm_bins_kernel<<<dim3(n_slices, n_draws), 1024, 0, st>>>(bargs);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "wpm_bins_kernel");
+  {
+    const ProfToken tok = prof_begin(WAP_KIND_WPM_BINS, st);
+    count_launch();
+    wpm_bins_kernel<<<dim3(n_slices, n_draws), 1024, 0, st>>>(bargs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "wpm_bins_kernel");
+    prof_end(tok, st, 4.0 * plane * n_slices * n_draws);
+  }
 
   // psi0 -> row spectrum
   RowArgs r = base_row_args(p, ph, V, n_slices, draw);
@@ -140,18 +146,26 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
     for (int s = 0; s < n_slices; ++s) {
       c.slice = s;
       c.dp_mode = 0;
+      ProfToken tok = prof_begin(WAP_KIND_WPM_COL, st);
       if ((e = launch_wpm_col(p->ny, p->col_e, c, nb, p->col_w, st)) != cudaSuccess) return cuda_fail(e, "wpm column pass");
+      // wave in, K fields out, vacuum propagator once
+      prof_end(tok, st, (8.0 + 8.0 * K) * plane * nb + 8.0 * plane);
       w.slice = s;
       w.last = (s == n_slices - 1);
       w.snap = stack ? reinterpret_cast<float2*>(stack) + (long long)s * plane : nullptr;
+      tok = prof_begin(WAP_KIND_WPM_ROW, st);
       if ((e = launch_wpm_row(p->nx, p->row_e, w, nb, rows, st)) != cudaSuccess) return cuda_fail(e, "wpm row pass");
+      // K fields in, potential, wave out (+ dp buffer on the last slice, + snapshot)
+      prof_end(tok, st, (8.0 * K + 4.0 + 8.0 + (w.last ? 8.0 : 0.0) + (w.snap ? 8.0 : 0.0)) * plane * nb);
     }
     if (dp) {
       WpmColArgs d = c;
       d.psi = p->dpbuf;
       d.dp = dp;
       d.dp_mode = 1;
+      const ProfToken tok = prof_begin(WAP_KIND_WPM_COL, st);
       if ((e = launch_wpm_col(p->ny, p->col_e, d, nb, p->col_w, st)) != cudaSuccess) return cuda_fail(e, "wpm dp pass");
+      prof_end(tok, st, 12.0 * plane * nb);
     }
   }
   return WAP_OK;
