@@ -324,11 +324,11 @@ def _grad_ratio(args):
     from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
     w = wap.synthetic.inverse_problem(0)
     dev = torch.device("cuda", torch.cuda.current_device())
-    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy, dtype=torch.complex64)
+    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
     probe = torch.as_tensor(w.probe).to(dev)
     pos = torch.as_tensor(w.positions).to(dev)
     Vt = torch.as_tensor(w.potential[0]).to(dev)
-    _, target = wap.simulate_fresnel_as(Vt, probe, H, w.dz, w.energy, positions=pos, return_wavefronts=False)
+    _, target, _ = wap.simulate_fresnel_as(Vt, probe, H, w.dz, w.energy, positions=pos, return_wavefronts=False)
     V = torch.zeros_like(Vt, requires_grad=True)
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
@@ -386,8 +386,7 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world):
     host = []
     for w in classes_host:
         V = torch.from_numpy(w.potential).pin_memory()
-        H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy,
-                                                    dtype=torch.complex64)
+        H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
         host.append((w, V, torch.from_numpy(w.probe).pin_memory(), torch.from_numpy(w.positions).pin_memory(),
                      torch.from_numpy(w.draw_of_probe).pin_memory(), H,
                      torch.empty((w.n_probes, w.ny, w.nx), dtype=torch.float32).pin_memory()))

@@ -61,9 +61,11 @@ int wap_plan_get_config(const wap_plan* plan, int* row_e, int* col_e, int* col_w
  *   WAP_TF_ANGULAR: propagation.py:148-156
  *       H[i,j] = exp(i 2 pi z sqrt_c(1/lam^2 - fx_i^2 - fy_j^2))
  * with fx = fftfreq(n, ps0), fy = fftfreq(m, ps1) (meshgrid 'ij', shape n x m).
- * out is complex128 when out_c128 != 0, else complex64. */
+ * out is complex128 when out_c128 != 0, else complex64; for complex64, out_lo
+ * (nullable) receives the rounding remainder value - (complex64)value, the
+ * H_lo argument of the multislice calls. */
 int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double z,
-                          double energy, void* out, int out_c128, void* stream);
+                          double energy, void* out, int out_c128, void* out_lo, void* stream);
 
 /* Fresnel / angular-spectrum multislice forward, propagation.py:305-352.
  *   V        (n_draws, n_slices, ny, nx) float32 mean potential per slice [V]
@@ -73,6 +75,10 @@ int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double
  *   positions(n_probes, 2) int32 probe centres (row, col) applied like
  *            move_probe (propagation.py:263-276), or NULL (no shift)
  *   H        (ny, nx) complex64 transfer function
+ *   H_lo     (ny, nx) complex64 remainder H - (complex64)H of a float64
+ *            transfer function, or NULL.  The same rounding of H is applied
+ *            at every slice, so its error grows linearly with the slice count;
+ *            with H_lo the product is formed as X H + X H_lo.
  *   exit     (n_probes, ny, nx) complex64 out (also the working buffer)
  *   dp       (n_probes, ny, nx) float32 |fftshift(fft2(exit))|^2, or NULL
  *   stack    (n_probes, n_slices, ny, nx) complex64 wave after every slice,
@@ -81,8 +87,8 @@ int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double
 int wap_multislice_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
                        const int32_t* draw, const float* psi0, int n_probes,
                        int psi0_per_probe, const int32_t* positions, const float* H,
-                       double dz, double energy, float* exit, float* dp, float* stack,
-                       void* stream);
+                       const float* H_lo, double dz, double energy, float* exit, float* dp,
+                       float* stack, void* stream);
 
 /* WPM adaptive-binning multislice forward, propagation.py:358-387 with the
  * step of propagation.py:215-256 (n_bins reference indices spaced
@@ -110,12 +116,12 @@ int wap_wpm_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
 int wap_multislice_fwd_ckpt(wap_plan* plan, const float* V, int n_slices, int n_draws,
                             const int32_t* draw, const float* psi0, int n_probes,
                             int psi0_per_probe, const int32_t* positions, const float* H,
-                            double dz, double energy, float* exit, float* dp, float* ckpt,
-                            int ckpt_every, void* stream);
+                            const float* H_lo, double dz, double energy, float* exit, float* dp,
+                            float* ckpt, int ckpt_every, void* stream);
 
 int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws,
-                       const int32_t* draw, int n_probes, const float* H, double dz,
-                       double energy, const float* exit, const float* ckpt, int ckpt_every,
+                       const int32_t* draw, int n_probes, const float* H, const float* H_lo,
+                       double dz, double energy, const float* exit, const float* ckpt, int ckpt_every,
                        const float* grad_dp, const float* grad_exit, float* grad_V,
                        float* work, void* stream);
 

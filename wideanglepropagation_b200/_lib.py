@@ -36,11 +36,11 @@ SIGNATURES = {
     "wap_plan_destroy": (_I, [_P]),
     "wap_plan_set_config": (_I, [_P, _I, _I, _I]),
     "wap_plan_get_config": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
-    "wap_transfer_function": (_I, [_I, _I, _I, _D, _D, _D, _D, _P, _I, _P]),
-    "wap_multislice_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _D, _D, _P, _P, _P, _P]),
+    "wap_transfer_function": (_I, [_I, _I, _I, _D, _D, _D, _D, _P, _I, _P, _P]),
+    "wap_multislice_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "wap_wpm_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P]),
-    "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
-    "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
+    "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
     "wap_launch_count": (ctypes.c_longlong, []),
     "wap_profile_enable": (_I, [_I]),
     "wap_profile_reset": (_I, []),

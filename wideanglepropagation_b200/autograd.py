@@ -21,7 +21,7 @@ import math
 import torch
 
 from . import _lib
-from .propagation import _device, _prepare, _ptr, _stream, _to, get_plan
+from .propagation import _device, _prepare, _ptr, _stream, get_plan, split_transfer
 
 
 class MultisliceFunction(torch.autograd.Function):
@@ -29,7 +29,7 @@ class MultisliceFunction(torch.autograd.Function):
     def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every):
         dev = V.device
         Vc, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(V.detach(), probe, positions, draw, dev)
-        Hc = _to(H, torch.complex64, dev)
+        Hc, Hl = split_transfer(H, dev)
         plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
         k = max(1, int(ckpt_every))
         nck = (N + k - 1) // k
@@ -38,8 +38,11 @@ class MultisliceFunction(torch.autograd.Function):
         ckpt = torch.empty((B, nck, ny, nx), dtype=torch.complex64, device=dev)
         _lib.check(_lib.lib().wap_multislice_fwd_ckpt(
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
-            _ptr(pos), _ptr(Hc), float(dz), float(energy), _ptr(exit_wave), _ptr(dp), _ptr(ckpt), k, _stream()))
-        ctx.save_for_backward(Vc, Hc, exit_wave, ckpt, dr if dr is not None else torch.empty(0, device=dev))
+            _ptr(pos), _ptr(Hc), _ptr(Hl), float(dz), float(energy), _ptr(exit_wave), _ptr(dp), _ptr(ckpt), k,
+            _stream()))
+        empty = torch.empty(0, device=dev)
+        ctx.save_for_backward(Vc, Hc, Hl if Hl is not None else empty, exit_wave, ckpt,
+                              dr if dr is not None else empty)
         ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched)
         if not batched:
             return exit_wave[0], dp[0]
@@ -47,7 +50,7 @@ class MultisliceFunction(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_exit, g_dp):
-        Vc, Hc, exit_wave, ckpt, dr = ctx.saved_tensors
+        Vc, Hc, Hl, exit_wave, ckpt, dr = ctx.saved_tensors
         B, N, ny, nx, dz, energy, k, has_draw, vshape, batched = ctx.meta
         dev = Vc.device
         plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
@@ -58,7 +61,8 @@ class MultisliceFunction(torch.autograd.Function):
         grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=dev)
         work = torch.empty((B, k + 2, ny, nx), dtype=torch.complex64, device=dev)
         _lib.check(_lib.lib().wap_multislice_bwd(
-            plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr) if has_draw else None, B, _ptr(Hc), dz, energy,
+            plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr) if has_draw else None, B, _ptr(Hc),
+            _ptr(Hl) if Hl.numel() else None, dz, energy,
             _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
         return grad_V.reshape(vshape), None, None, None, None, None, None, None
 

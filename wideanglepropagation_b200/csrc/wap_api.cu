@@ -55,11 +55,11 @@ Physics physics(double energy, double dz) {
 
 // ----------------------------------------------------------------------------
 // twiddle tables: per Stockham stage s >= 1, W_{L R}^{j k} laid out [j][k],
-// from float64 sin/cos rounded once to float32
+// each float64 value stored as float hi + lo parts (re_hi, im_hi, re_lo, im_lo)
 // ----------------------------------------------------------------------------
-std::vector<float2> twiddle_table(int n, int e) {
+std::vector<float4> twiddle_table(int n, int e) {
   const PlanShape p = make_plan_shape(n, e);
-  std::vector<float2> tw(p.tw_size(), make_float2(1.f, 0.f));
+  std::vector<float4> tw(p.tw_size(), make_float4(1.f, 0.f, 0.f, 0.f));
   for (int s = 1; s < p.stages; ++s) {
     const int R = p.radix(s), L = p.span(s), off = p.tw_offset(s);
     const long long LR = (long long)L * R;
@@ -67,7 +67,9 @@ std::vector<float2> twiddle_table(int n, int e) {
       for (int k = 0; k < L; ++k) {
         const long long m = ((long long)j * k) % LR;
         const double ang = -2.0 * M_PI * (double)m / (double)LR;
-        tw[off + j * L + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        const double c = std::cos(ang), sn = std::sin(ang);
+        const float ch = (float)c, sh = (float)sn;
+        tw[off + j * L + k] = make_float4(ch, sh, (float)(c - (double)ch), (float)(sn - (double)sh));
       }
   }
   return tw;
@@ -84,12 +86,12 @@ static cudaError_t prep_smem(K kern, size_t smem) {
 
 template <int N, int E>
 size_t row_smem_bytes(int rows, int extra_bytes) {
-  return (size_t)rows * RowCfg<N, E>::PADN * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float2) + extra_bytes;
+  return (size_t)rows * RowCfg<N, E>::PADN * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float4) + extra_bytes;
 }
 
 template <int N, int E>
 size_t col_smem_bytes(int w, int extra_bytes) {
-  return (size_t)N * w * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float2) + extra_bytes;
+  return (size_t)N * w * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float4) + extra_bytes;
 }
 
 template <int N, int E>
@@ -105,10 +107,17 @@ static cudaError_t launch_row_t(const RowArgs& a, int nb, int rows, cudaStream_t
 template <int N, int E>
 static cudaError_t launch_col_t(const ColArgs& a, int nb, int w, cudaStream_t st) {
   const size_t smem = col_smem_bytes<N, E>(w, 0);
-  cudaError_t err = prep_smem(col_pass_kernel<N, E>, smem);
-  if (err != cudaSuccess) return err;
+  const dim3 grid(a.nx / w, nb);
+  const int threads = w * FFTPlan<N, E>::T;
+  cudaError_t err;
   count_launch();
-  col_pass_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
+  if (a.flags & COL_SEED) {
+    if ((err = prep_smem(col_pass_kernel<N, E, true>, smem)) != cudaSuccess) return err;
+    col_pass_kernel<N, E, true><<<grid, threads, smem, st>>>(a);
+  } else {
+    if ((err = prep_smem(col_pass_kernel<N, E, false>, smem)) != cudaSuccess) return err;
+    col_pass_kernel<N, E, false><<<grid, threads, smem, st>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -173,6 +182,7 @@ struct TfArgs {
   int kind, n, m, c128;
   double ps0, ps1, z, lambda;
   void* out;
+  float2* out_lo;   // complex64 output only: value - (complex64)value, or null
 };
 
 // out[i, j], i < n (axis 0, fftfreq(n, ps0)), j < m (axis 1, fftfreq(m, ps1))
@@ -201,7 +211,9 @@ __global__ void transfer_kernel(const TfArgs a) {
   if (a.c128) {
     reinterpret_cast<double2*>(a.out)[idx] = make_double2(re, im);
   } else {
-    reinterpret_cast<float2*>(a.out)[idx] = make_float2((float)re, (float)im);
+    const float rh = (float)re, ih = (float)im;
+    reinterpret_cast<float2*>(a.out)[idx] = make_float2(rh, ih);
+    if (a.out_lo) a.out_lo[idx] = make_float2((float)(re - (double)rh), (float)(im - (double)ih));
   }
 }
 
@@ -216,13 +228,13 @@ static int upload_twiddles(wap_plan* p) {
   for (int which = 0; which < 2; ++which) {
     const int n = which == 0 ? p->nx : p->ny;
     const int e = which == 0 ? p->row_e : p->col_e;
-    std::vector<float2> h = twiddle_table(n, e);
-    float2*& d = which == 0 ? p->tw_row : p->tw_col;
+    std::vector<float4> h = twiddle_table(n, e);
+    float4*& d = which == 0 ? p->tw_row : p->tw_col;
     if (d) cudaFree(d);
     d = nullptr;
-    cudaError_t err = cudaMalloc(&d, h.size() * sizeof(float2));
+    cudaError_t err = cudaMalloc(&d, h.size() * sizeof(float4));
     if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(twiddles)");
-    err = cudaMemcpy(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    err = cudaMemcpy(d, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) return cuda_fail(err, "cudaMemcpy(twiddles)");
   }
   return WAP_OK;
@@ -281,6 +293,7 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
     cudaError_t err = cudaMalloc(&p->fields, (size_t)max_batch * n_bins * plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->dpbuf, (size_t)max_batch * plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->hvac, plane * sizeof(float2));
+    if (err == cudaSuccess) err = cudaMalloc(&p->hvac_lo, plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->ky2, ny * sizeof(float));
     if (err == cudaSuccess) err = cudaMalloc(&p->kx2, nx * sizeof(float));
     if (err != cudaSuccess) {
@@ -300,6 +313,7 @@ int wap_plan_destroy(wap_plan* p) {
   cudaFree(p->fields);
   cudaFree(p->dpbuf);
   cudaFree(p->hvac);
+  cudaFree(p->hvac_lo);
   cudaFree(p->ky2);
   cudaFree(p->kx2);
   cudaFree(p->refs);
@@ -329,13 +343,15 @@ int wap_plan_get_config(const wap_plan* p, int* row_e, int* col_e, int* col_w) {
 }
 
 int wap_transfer_function(int kind, int n, int m, double ps0, double ps1, double z, double energy, void* out,
-                          int out_c128, void* stream) {
+                          int out_c128, void* out_lo, void* stream) {
   clear_error();
   if (!out) return fail(WAP_ERR_ARG, "out is NULL");
   if (kind != WAP_TF_FRESNEL && kind != WAP_TF_ANGULAR) return fail(WAP_ERR_ARG, "unknown transfer function %d", kind);
   if (n < 1 || m < 1) return fail(WAP_ERR_ARG, "bad shape %d x %d", n, m);
   if (!(energy > 0) || !(ps0 > 0) || !(ps1 > 0)) return fail(WAP_ERR_ARG, "energy and sampling must be positive");
-  TfArgs a{kind, n, m, out_c128 ? 1 : 0, ps0, ps1, z, physics(energy, 1.0).lambda, out};
+  if (out_c128 && out_lo) return fail(WAP_ERR_ARG, "out_lo is only produced with a complex64 out");
+  TfArgs a{kind, n, m, out_c128 ? 1 : 0, ps0, ps1, z, physics(energy, 1.0).lambda, out,
+           reinterpret_cast<float2*>(out_lo)};
   const long long total = (long long)n * m;
   count_launch();
   transfer_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
@@ -381,9 +397,10 @@ RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int 
   return r;
 }
 
-ColArgs base_col_args(const wap_plan* p, const float* H) {
+ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo) {
   ColArgs c{};
   c.H = reinterpret_cast<const float2*>(H);
+  c.H_lo = reinterpret_cast<const float2*>(H_lo);
   c.tw = p->tw_col;
   c.ny = p->ny;
   c.nx = p->nx;
@@ -437,7 +454,8 @@ cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t 
 // snap + (s / snap_every) * plane when s % snap_every == 0 (snap_first = 0:
 // checkpoints), or the wave after every slice to stack (snap_first = 1).
 int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, const float* psi0,
-                    int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, double dz,
+                    int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, const float* H_lo,
+                    double dz,
                     double energy, float* exit, float* dp, float* stack, float* ckpt, int ckpt_every,
                     cudaStream_t st) {
   int rc = check_common(p, V, n_slices, n_draws, psi0, n_probes, exit);
@@ -454,7 +472,7 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   r.src = reinterpret_cast<const float2*>(psi0);
   r.src_bstride = psi0_per_probe ? plane : 0;
   r.shifts = positions;
-  ColArgs c = base_col_args(p, H);
+  ColArgs c = base_col_args(p, H, H_lo);
   c.psi = r.psi;
   c.psi_bstride = plane;
   c.dp = dp;
@@ -485,29 +503,30 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
 extern "C" {
 
 int wap_multislice_fwd(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, const float* psi0,
-                       int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, double dz,
-                       double energy, float* exit, float* dp, float* stack, void* stream) {
+                       int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, const float* H_lo,
+                       double dz, double energy, float* exit, float* dp, float* stack, void* stream) {
   clear_error();
-  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, dz, energy, exit,
-                         dp, stack, nullptr, 1, (cudaStream_t)stream);
+  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, H_lo, dz, energy,
+                         exit, dp, stack, nullptr, 1, (cudaStream_t)stream);
 }
 
 int wap_multislice_fwd_ckpt(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw,
                             const float* psi0, int n_probes, int psi0_per_probe, const int32_t* positions,
-                            const float* H, double dz, double energy, float* exit, float* dp, float* ckpt,
-                            int ckpt_every, void* stream) {
+                            const float* H, const float* H_lo, double dz, double energy, float* exit, float* dp,
+                            float* ckpt, int ckpt_every, void* stream) {
   clear_error();
   if (!ckpt) return fail(WAP_ERR_ARG, "ckpt must be a non-NULL device pointer");
   if (ckpt_every < 1) return fail(WAP_ERR_ARG, "ckpt_every must be >= 1");
-  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, dz, energy, exit,
-                         dp, nullptr, ckpt, ckpt_every, (cudaStream_t)stream);
+  return fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, H_lo, dz, energy,
+                         exit, dp, nullptr, ckpt, ckpt_every, (cudaStream_t)stream);
 }
 
 // ----------------------------------------------------------------------------
 // adjoint (gradient w.r.t. V)
 // ----------------------------------------------------------------------------
 int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, int n_probes,
-                       const float* H, double dz, double energy, const float* exit, const float* ckpt, int ckpt_every,
+                       const float* H, const float* H_lo, double dz, double energy, const float* exit, const float* ckpt,
+                       int ckpt_every,
                        const float* grad_dp, const float* grad_exit, float* grad_V, float* work, void* stream) {
   clear_error();
   int rc = check_common(p, V, n_slices, n_draws, exit, n_probes, const_cast<float*>(exit));
@@ -546,7 +565,7 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
     if ((e = row_chunks(p, r, n_probes, st)) != cudaSuccess) return cuda_fail(e, "seed row pass");
     r.src_scale = 1.0f;
   }
-  ColArgs c = base_col_args(p, H);
+  ColArgs c = base_col_args(p, H, H_lo);
   c.psi = lam;
   c.psi_bstride = wstride;
   c.flags = COL_SEED | COL_CONJ_H;
@@ -573,7 +592,7 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
         q.snap_bstride = wstride;
       }
       if ((e = row_chunks(p, q, n_probes, st)) != cudaSuccess) return cuda_fail(e, "recompute row pass");
-      ColArgs cc = base_col_args(p, H);
+      ColArgs cc = base_col_args(p, H, H_lo);
       cc.psi = buf;
       cc.psi_bstride = wstride;
       if ((e = col_chunks(p, cc, n_probes, st)) != cudaSuccess) return cuda_fail(e, "recompute column pass");
@@ -605,7 +624,7 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
       a.grad = grad_V;
       if ((e = row_chunks(p, a, n_probes, st)) != cudaSuccess) return cuda_fail(e, "adjoint row pass");
       if (s == 0) break;
-      ColArgs ca = base_col_args(p, H);
+      ColArgs ca = base_col_args(p, H, H_lo);
       ca.psi = lam;
       ca.psi_bstride = wstride;
       ca.flags = COL_CONJ_H;

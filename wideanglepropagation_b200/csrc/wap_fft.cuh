@@ -10,7 +10,9 @@
 // b = t + T*q, k = b mod L:
 //   inputs  x[b + (N/R) j] = register slot q + (E/R) j
 //   twiddle W_{LR}^{jk}, from a per-stage table laid out [j][k] so that
-//           consecutive threads read consecutive words
+//           consecutive threads read consecutive words; each entry holds
+//           the float64 value as float hi + lo parts (systematic rounding
+//           of a float-only table would repeat identically every slice)
 //   outputs y_m -> position (b - k) R + k + m L, exchanged through shared
 //           memory for every stage but the last.
 // After the last stage thread t again holds X[t + T*e] in slot e, so a forward
@@ -102,31 +104,40 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
   return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-// cos / sin of 2 pi m / 16, exact to float rounding
-__device__ __forceinline__ float cos16(int m) {
+// cos / sin of 2 pi m / 16 as an unevaluated float sum hi + lo (|lo| < ulp(hi)/2).
+// The hi parts alone carry a systematic rounding error that every slice
+// applies again; the lo parts remove it (see tw16).
+struct Pair {
+  float hi, lo;
+};
+__device__ __forceinline__ Pair cos16p(int m) {
+  constexpr float C8H = 0.9238795042037964f, C8L = 2.830748968563057e-08f;
+  constexpr float R2H = 0.7071067690849304f, R2L = 1.2101617485882343e-08f;
+  constexpr float S8H = 0.3826834261417389f, S8L = 6.2233507236442165e-09f;
   switch (m & 15) {
-    case 0: return 1.0f;
-    case 1: return 0.92387953251128674f;
-    case 2: return 0.70710678118654752f;
-    case 3: return 0.38268343236508977f;
-    case 4: return 0.0f;
-    case 5: return -0.38268343236508977f;
-    case 6: return -0.70710678118654752f;
-    case 7: return -0.92387953251128674f;
-    case 8: return -1.0f;
-    case 9: return -0.92387953251128674f;
-    case 10: return -0.70710678118654752f;
-    case 11: return -0.38268343236508977f;
-    case 12: return 0.0f;
-    case 13: return 0.38268343236508977f;
-    case 14: return 0.70710678118654752f;
-    default: return 0.92387953251128674f;
+    case 0: return {1.0f, 0.0f};
+    case 1: return {C8H, C8L};
+    case 2: return {R2H, R2L};
+    case 3: return {S8H, S8L};
+    case 4: return {0.0f, 0.0f};
+    case 5: return {-S8H, -S8L};
+    case 6: return {-R2H, -R2L};
+    case 7: return {-C8H, -C8L};
+    case 8: return {-1.0f, 0.0f};
+    case 9: return {-C8H, -C8L};
+    case 10: return {-R2H, -R2L};
+    case 11: return {-S8H, -S8L};
+    case 12: return {0.0f, 0.0f};
+    case 13: return {S8H, S8L};
+    case 14: return {R2H, R2L};
+    default: return {C8H, C8L};
   }
 }
-__device__ __forceinline__ float sin16(int m) { return cos16(m - 4); }
+__device__ __forceinline__ Pair sin16p(int m) { return cos16p(m - 4); }
 
 // a * W16^m with W16 = exp(-+2 pi i / 16); m is a compile-time constant after
-// unrolling, so the branches fold away.
+// unrolling, so the branches fold away.  Non-trivial constants are applied as
+// hi + lo through FMAs.
 template <bool INV>
 __device__ __forceinline__ float2 tw16(float2 a, int m) {
   m &= 15;
@@ -134,14 +145,37 @@ __device__ __forceinline__ float2 tw16(float2 a, int m) {
   if (m == 8) return make_float2(-a.x, -a.y);
   if (m == 4) return mul_mi<INV>(a);
   if (m == 12) return mul_mi<!INV>(a);
-  const float c = cos16(m);
-  const float s = INV ? sin16(m) : -sin16(m);  // twiddle = c + i s
+  const Pair c = cos16p(m);
+  Pair s = sin16p(m);
+  if (!INV) s = {-s.hi, -s.lo};  // twiddle = c + i s
   if ((m & 3) == 2) {
-    // |c| == |s|: two adds, two multiplies
-    if (c == s) return make_float2(c * (a.x - a.y), c * (a.y + a.x));
-    return make_float2(c * (a.x + a.y), c * (a.y - a.x));
+    // |c| == |s|: one rounded sum, then c (hi + lo)
+    const float d0 = (c.hi == s.hi) ? a.x - a.y : a.x + a.y;
+    const float d1 = (c.hi == s.hi) ? a.y + a.x : a.y - a.x;
+    return make_float2(fmaf(c.hi, d0, c.lo * d0), fmaf(c.hi, d1, c.lo * d1));
   }
-  return make_float2(fmaf(c, a.x, -s * a.y), fmaf(c, a.y, s * a.x));
+  return make_float2(fmaf(c.hi, a.x, fmaf(-s.hi, a.y, fmaf(c.lo, a.x, -s.lo * a.y))),
+                     fmaf(c.hi, a.y, fmaf(s.hi, a.x, fmaf(c.lo, a.y, s.lo * a.x))));
+}
+
+// complex multiply by a twiddle stored as (re_hi, im_hi, re_lo, im_lo)
+__device__ __forceinline__ float2 cmul_tw(float2 a, float4 w) {
+  return make_float2(fmaf(a.x, w.x, fmaf(-a.y, w.y, fmaf(a.x, w.z, -a.y * w.w))),
+                     fmaf(a.x, w.y, fmaf(a.y, w.x, fmaf(a.x, w.w, a.y * w.z))));
+}
+// a * conj(twiddle)
+__device__ __forceinline__ float2 cmulc_tw(float2 a, float4 w) {
+  return make_float2(fmaf(a.x, w.x, fmaf(a.y, w.y, fmaf(a.x, w.z, a.y * w.w))),
+                     fmaf(a.y, w.x, fmaf(-a.x, w.y, fmaf(a.y, w.z, -a.x * w.w))));
+}
+// a * (h + hl) for a propagator value split into complex64 hi and lo parts
+__device__ __forceinline__ float2 cmul_hl(float2 a, float2 h, float2 hl) {
+  return make_float2(fmaf(a.x, h.x, fmaf(-a.y, h.y, fmaf(a.x, hl.x, -a.y * hl.y))),
+                     fmaf(a.x, h.y, fmaf(a.y, h.x, fmaf(a.x, hl.y, a.y * hl.x))));
+}
+__device__ __forceinline__ float2 cmulc_hl(float2 a, float2 h, float2 hl) {
+  return make_float2(fmaf(a.x, h.x, fmaf(a.y, h.y, fmaf(a.x, hl.x, a.y * hl.y))),
+                     fmaf(a.y, h.x, fmaf(-a.x, h.y, fmaf(a.y, hl.x, -a.x * hl.y))));
 }
 
 // ----------------------------------------------------------------------------
@@ -244,7 +278,7 @@ struct ColExchange {
 // Stockham stages
 // ----------------------------------------------------------------------------
 template <int N, int E, int SI, bool INV, class X>
-__device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, const float4* __restrict__ tw) {
   using P = FFTPlan<N, E>;
   constexpr int R = P::radix(SI);
   constexpr int L = P::span(SI);
@@ -262,8 +296,8 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
     if constexpr (L > 1) {
 #pragma unroll
       for (int j = 1; j < R; ++j) {
-        const float2 w = tw[OFF + j * L + k];
-        a[j] = INV ? cmulc(a[j], w) : cmul(a[j], w);
+        const float4 w = tw[OFF + j * L + k];
+        a[j] = INV ? cmulc_tw(a[j], w) : cmul_tw(a[j], w);
       }
     }
     dft<R, INV>(a);
@@ -287,7 +321,7 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
 }
 
 template <int N, int E, bool INV, class X, int SI = 0>
-__device__ __forceinline__ void fft(float2 (&v)[E], int t, const X& xs, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft(float2 (&v)[E], int t, const X& xs, const float4* __restrict__ tw) {
   if constexpr (SI < FFTPlan<N, E>::S) {
     fft_stage<N, E, SI, INV>(v, t, xs, tw);
     fft<N, E, INV, X, SI + 1>(v, t, xs, tw);

@@ -11,12 +11,13 @@ struct wap_plan {
   int device = 0;
   int ny = 0, nx = 0, max_batch = 0, op = 0, n_bins = 0;
   int row_e = 16, col_e = 16, col_w = 16;   // FFT launch shape (autotuned)
-  float2* tw_row = nullptr;                 // twiddles for nx / row_e
-  float2* tw_col = nullptr;                 // twiddles for ny / col_e
+  float4* tw_row = nullptr;                 // twiddles for nx / row_e (hi, lo)
+  float4* tw_col = nullptr;                 // twiddles for ny / col_e (hi, lo)
   // WPM workspace
   float2* fields = nullptr;                 // (max_batch, n_bins, ny, nx)
   float2* dpbuf = nullptr;                  // (max_batch, ny, nx)
-  float2* hvac = nullptr;                   // (ny, nx)
+  float2* hvac = nullptr;                   // (ny, nx) hi part
+  float2* hvac_lo = nullptr;                // (ny, nx) lo part
   float* ky2 = nullptr;
   float* kx2 = nullptr;
   double hvac_key[4] = {0, 0, 0, 0};        // (dy, dx, dz, energy) of hvac
@@ -31,7 +32,7 @@ struct Physics {
 };
 
 Physics physics(double energy, double dz);
-std::vector<float2> twiddle_table(int n, int e);
+std::vector<float4> twiddle_table(int n, int e);
 
 int fail(int code, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);

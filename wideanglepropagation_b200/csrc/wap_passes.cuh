@@ -59,7 +59,7 @@ struct RowArgs {
   const float* V;            // (draws, n_slices, ny, nx) volts
   const int* draw;           // (B) potential draw per probe, or null
   long long v_draw_stride;   // n_slices * ny * nx
-  const float2* tw;          // twiddle table for nx
+  const float4* tw;          // twiddle table for nx (hi, lo)
   float2* snap;              // snapshot of the spatial wave entering `slice`
   long long snap_bstride;    //   (after the load / inverse FFT), or null
   const float2* aux;         // ROW_ADJOINT: forward wave psi_s entering slice s
@@ -80,7 +80,8 @@ struct ColArgs {
   float2* psi;
   long long psi_bstride;
   const float2* H;           // (ny, nx)
-  const float2* tw;          // twiddle table for ny
+  const float2* H_lo;        // (ny, nx) H - H rounded to complex64, or null
+  const float4* tw;          // twiddle table for ny (hi, lo)
   float* dp;                 // COL_DP: (B, ny, nx)
   const float* g;            // COL_SEED: dL/ddp (B, ny, nx), fftshifted like dp
   const float2* seed2;       // COL_SEED: optional row-transformed lambda_exit
@@ -132,8 +133,8 @@ row_pass_kernel(const RowArgs a) {
   constexpr int T = C::T;
   const int rows = blockDim.x / T;
   extern __shared__ float4 smem_raw[];
-  float2* xbuf = reinterpret_cast<float2*>(smem_raw);
-  float2* tw = xbuf + rows * C::PADN;
+  float4* tw = smem_raw;
+  float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
   for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
@@ -223,17 +224,44 @@ row_pass_kernel(const RowArgs a) {
 }
 
 // ----------------------------------------------------------------------------
+// column tiles: [NY][W] complex64 between global memory (row stride nx) and
+// shared memory, 16 bytes per access; consecutive threads take consecutive
+// 16-byte words of a row segment, so a warp moves 512 contiguous-by-row bytes.
+// ----------------------------------------------------------------------------
+template <int NY>
+__device__ __forceinline__ void tile_load(float2* tile, const float2* __restrict__ g, int W, int nx) {
+  const int w2 = W >> 1;
+  const int sh = __ffs(w2) - 1;
+  float4* t4 = reinterpret_cast<float4*>(tile);
+  for (int i = threadIdx.x; i < NY * w2; i += blockDim.x) {
+    const int r = i >> sh, c2 = i & (w2 - 1);
+    t4[i] = __ldcg(reinterpret_cast<const float4*>(g + (long long)r * nx) + c2);
+  }
+}
+
+template <int NY>
+__device__ __forceinline__ void tile_store(float2* __restrict__ g, const float2* tile, int W, int nx) {
+  const int w2 = W >> 1;
+  const int sh = __ffs(w2) - 1;
+  const float4* t4 = reinterpret_cast<const float4*>(tile);
+  for (int i = threadIdx.x; i < NY * w2; i += blockDim.x) {
+    const int r = i >> sh, c2 = i & (w2 - 1);
+    __stcg(reinterpret_cast<float4*>(g + (long long)r * nx) + c2, t4[i]);
+  }
+}
+
+// ----------------------------------------------------------------------------
 // column pass
 // ----------------------------------------------------------------------------
-template <int NY, int E>
+template <int NY, int E, bool SEED>
 __global__ void __launch_bounds__(kColThreads)
 col_pass_kernel(const ColArgs a) {
   using P = FFTPlan<NY, E>;
   constexpr int T = P::T;
   const int W = blockDim.x / T;
   extern __shared__ float4 smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);
-  float2* tw = tile + NY * W;
+  float4* tw = smem_raw;
+  float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
   for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
@@ -243,31 +271,35 @@ col_pass_kernel(const ColArgs a) {
   const int b = a.probe0 + blockIdx.y;
   const int nx = a.nx;
   const long long plane = (long long)NY * nx;
-  float2* pcol = a.psi + (long long)b * a.psi_bstride + col;
+  float2* ptile = a.psi + (long long)b * a.psi_bstride + (long long)blockIdx.x * W;
   const ColExchange xs{tile, W, c};
   const int f = a.flags;
 
   float2 v[E];
+  tile_load<NY>(tile, ptile, W, nx);
+  __syncthreads();
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = __ldcg(pcol + (long long)(t + T * e) * nx);
+  for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
 
   fft<NY, E, false>(v, t, xs, tw);
 
   // fftshift of (ky, kx) for dp / g
   const int sx = (col + (nx >> 1)) & (nx - 1);
-  if (f & COL_SEED) {
+  if constexpr (SEED) {
     const float* gp = a.g + (long long)b * plane;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int ky = t + T * e;
       const int sy = (ky + (NY >> 1)) & (NY - 1);
-      v[e] = cscale(v[e], a.seed_scale * __ldg(gp + (long long)sy * nx + sx));
+      v[e] = a.g ? cscale(v[e], a.seed_scale * __ldg(gp + (long long)sy * nx + sx)) : make_float2(0.f, 0.f);
     }
     if (a.seed2) {
       float2 u[E];
-      const float2* s2 = a.seed2 + (long long)b * a.seed2_bstride + col;
+      __syncthreads();
+      tile_load<NY>(tile, a.seed2 + (long long)b * a.seed2_bstride + (long long)blockIdx.x * W, W, nx);
+      __syncthreads();
 #pragma unroll
-      for (int e = 0; e < E; ++e) u[e] = __ldcg(s2 + (long long)(t + T * e) * nx);
+      for (int e = 0; e < E; ++e) u[e] = xs.ld(t + T * e);
       fft<NY, E, false>(u, t, xs, tw);
 #pragma unroll
       for (int e = 0; e < E; ++e) v[e] = cadd(v[e], u[e]);
@@ -276,7 +308,22 @@ col_pass_kernel(const ColArgs a) {
 
   if (!(f & COL_NO_H)) {
     const float2* hcol = a.H + col;
-    if (f & COL_CONJ_H) {
+    if (a.H_lo) {
+      const float2* lcol = a.H_lo + col;
+      if (f & COL_CONJ_H) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const long long o = (long long)(t + T * e) * nx;
+          v[e] = cmulc_hl(v[e], __ldg(hcol + o), __ldg(lcol + o));
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const long long o = (long long)(t + T * e) * nx;
+          v[e] = cmul_hl(v[e], __ldg(hcol + o), __ldg(lcol + o));
+        }
+      }
+    } else if (f & COL_CONJ_H) {
 #pragma unroll
       for (int e = 0; e < E; ++e) v[e] = cmulc(v[e], __ldg(hcol + (long long)(t + T * e) * nx));
     } else {
@@ -298,8 +345,11 @@ col_pass_kernel(const ColArgs a) {
 
   fft<NY, E, true>(v, t, xs, tw);
 
+  __syncthreads();
 #pragma unroll
-  for (int e = 0; e < E; ++e) __stcg(pcol + (long long)(t + T * e) * nx, v[e]);
+  for (int e = 0; e < E; ++e) xs.st(t + T * e, v[e]);
+  __syncthreads();
+  tile_store<NY>(ptile, tile, W, nx);
 }
 
 // ----------------------------------------------------------------------------
@@ -376,12 +426,13 @@ static __global__ void __launch_bounds__(1024) wpm_bins_kernel(const WpmBinsArgs
 struct WpmColArgs {
   const float2* psi;         // (B, ny, nx) row-transformed wave
   float2* fields;            // (B, K, ny, nx) column-transformed reference fields
-  const float2* hvac;        // (ny, nx)  exp(i dz kz_vac), float64-rounded
+  const float2* hvac;        // (ny, nx)  exp(i dz kz_vac): complex64 hi part
+  const float2* hvac_lo;     // (ny, nx)  and lo part of the float64 value
   const float* ky2;          // (ny) (2 pi fy)^2
   const float* kx2;          // (nx) (2 pi fx)^2
   const float* refs;         // (draws, n_slices, K)
   const int* draw;
-  const float2* tw;
+  const float4* tw;
   float* dp;                 // dp mode: |fft2|^2 (fftshifted), no fields
   int ny, nx, K, slice, n_slices, probe0, dp_mode;
   float k02;                 // k0^2
@@ -395,9 +446,9 @@ wpm_col_kernel(const WpmColArgs a) {
   constexpr int T = P::T;
   const int W = blockDim.x / T;
   extern __shared__ float4 smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);
-  float2* tw = tile + NY * W;
-  float* srefs = reinterpret_cast<float*>(tw + P::TW_SIZE);
+  float4* tw = smem_raw;
+  float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
+  float* srefs = reinterpret_cast<float*>(tile + NY * W);
   for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   const int c = threadIdx.x % W;
   const int t = threadIdx.x / W;
@@ -414,9 +465,10 @@ wpm_col_kernel(const WpmColArgs a) {
   const ColExchange xs{tile, W, c};
 
   float2 v[E];
-  const float2* pcol = a.psi + (long long)b * plane + col;
+  tile_load<NY>(tile, a.psi + (long long)b * plane + (long long)blockIdx.x * W, W, nx);
+  __syncthreads();
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = __ldcg(pcol + (long long)(t + T * e) * nx);
+  for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
   fft<NY, E, false>(v, t, xs, tw);
 
   if (a.dp_mode) {
@@ -437,13 +489,13 @@ wpm_col_kernel(const WpmColArgs a) {
   for (int e = 0; e < E; ++e) {
     const int ky = t + T * e;
     q0[e] = a.k02 - (__ldg(a.ky2 + ky) + kx2);
-    v[e] = cmul(v[e], __ldg(a.hvac + (long long)ky * nx + col));
+    v[e] = cmul_hl(v[e], __ldg(a.hvac + (long long)ky * nx + col), __ldg(a.hvac_lo + (long long)ky * nx + col));
   }
   float sq0[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) sq0[e] = sqrtf(fabsf(q0[e]));
 
-  float2* fcol = a.fields + (long long)b * a.K * plane + col;
+  float2* ftile = a.fields + (long long)b * a.K * plane + (long long)blockIdx.x * W;
   for (int k = 0; k < a.K; ++k) {
     const float dk = srefs[k];
     const float ak = a.k02 * dk * (2.0f + dk);   // n_k^2 k0^2 - k0^2
@@ -479,9 +531,11 @@ wpm_col_kernel(const WpmColArgs a) {
       }
     }
     fft<NY, E, true>(u, t, xs, tw);
-    float2* fk = fcol + (long long)k * plane;
+    __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; ++e) __stcg(fk + (long long)(t + T * e) * nx, u[e]);
+    for (int e = 0; e < E; ++e) xs.st(t + T * e, u[e]);
+    __syncthreads();
+    tile_store<NY>(ftile + (long long)k * plane, tile, W, nx);
   }
 }
 
@@ -494,7 +548,7 @@ struct WpmRowArgs {
   const int* draw;
   long long v_draw_stride;
   const float* refs;
-  const float2* tw;
+  const float4* tw;
   float2* snap;              // wavefront after this slice (spatial)
   long long snap_bstride;
   int ny, nx, K, slice, n_slices, probe0, last;
@@ -509,9 +563,9 @@ wpm_row_kernel(const WpmRowArgs a) {
   constexpr int T = C::T;
   const int rows = blockDim.x / T;
   extern __shared__ float4 smem_raw[];
-  float2* xbuf = reinterpret_cast<float2*>(smem_raw);
-  float2* tw = xbuf + rows * C::PADN;
-  float* srefs = reinterpret_cast<float*>(tw + C::P::TW_SIZE);
+  float4* tw = smem_raw;
+  float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
+  float* srefs = reinterpret_cast<float*>(xbuf + rows * C::PADN);
   unsigned* used = reinterpret_cast<unsigned*>(srefs + a.K);
   const int b = a.probe0 + blockIdx.y;
   const int d = a.draw ? a.draw[b] : 0;

@@ -24,6 +24,7 @@ struct HvacArgs {
   int ny, nx;
   double dy, dx, dz, k0;
   float2* hvac;
+  float2* hvac_lo;
   float* ky2;
   float* kx2;
 };
@@ -42,7 +43,9 @@ __global__ void wpm_vacuum_kernel(const HvacArgs a) {
     re = exp(-a.dz * sqrt(-q));
     im = 0.0;
   }
-  a.hvac[idx] = make_float2((float)re, (float)im);
+  const float rh = (float)re, ih = (float)im;
+  a.hvac[idx] = make_float2(rh, ih);
+  a.hvac_lo[idx] = make_float2((float)(re - (double)rh), (float)(im - (double)ih));
   if (ix == 0) a.ky2[iy] = (float)(ky * ky);
   if (iy == 0) a.kx2[ix] = (float)(kx * kx);
 }
@@ -77,7 +80,7 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
   }
   const double key[4] = {sampling_y, sampling_x, dz, energy};
   if (!std::equal(key, key + 4, p->hvac_key)) {
-    HvacArgs h{p->ny, p->nx, sampling_y, sampling_x, dz, ph.k0, p->hvac, p->ky2, p->kx2};
+    HvacArgs h{p->ny, p->nx, sampling_y, sampling_x, dz, ph.k0, p->hvac, p->hvac_lo, p->ky2, p->kx2};
     count_launch();
     wpm_vacuum_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(h);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "wpm_vacuum_kernel");
@@ -107,6 +110,7 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
   c.psi = reinterpret_cast<const float2*>(exit);
   c.fields = p->fields;
   c.hvac = p->hvac;
+  c.hvac_lo = p->hvac_lo;
   c.ky2 = p->ky2;
   c.kx2 = p->kx2;
   c.refs = p->refs;

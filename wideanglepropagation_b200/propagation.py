@@ -63,6 +63,22 @@ def _to(x, dtype, device) -> torch.Tensor:
     return x.to(device=device, dtype=dtype).contiguous()
 
 
+def split_transfer(H, device):
+    """complex64 hi part and remainder of a transfer function.
+
+    A complex128 H is split into H_hi = (complex64)H and H_lo = H - H_hi; the
+    kernels apply X*H_hi + X*H_lo, which removes the rounding of H that would
+    otherwise repeat identically at every slice.  A complex64 H has no lo part.
+    """
+    t = H if isinstance(H, torch.Tensor) else torch.as_tensor(np.asarray(H))
+    if t.dtype == torch.complex128:
+        t = t.to(device)
+        hi = t.to(torch.complex64)
+        lo = (t - hi.to(torch.complex128)).to(torch.complex64)
+        return hi.contiguous(), lo.contiguous()
+    return _to(t, torch.complex64, device), None
+
+
 def _ptr(t: Optional[torch.Tensor]):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
@@ -194,13 +210,24 @@ def shift_kernel(x0, y0, Fx, Fy):
 # transfer functions (propagation.py:139-156), float64 on the device
 # ---------------------------------------------------------------------------
 def _transfer(kind: int, n: int, m: int, ps, z: float, energy: float,
-              dtype=torch.complex128) -> torch.Tensor:
+              dtype=torch.complex128, with_lo: bool = False):
     dev = _device()
     p0, p1 = _pair(ps)
     out = torch.empty((int(n), int(m)), dtype=dtype, device=dev)
+    lo = torch.empty((int(n), int(m)), dtype=torch.complex64, device=dev) if with_lo else None
+    if with_lo and dtype != torch.complex64:
+        raise ValueError("with_lo needs dtype=torch.complex64")
     _lib.check(_lib.lib().wap_transfer_function(kind, int(n), int(m), p0, p1, float(z), float(energy),
-                                                _ptr(out), 1 if dtype == torch.complex128 else 0, _stream()))
-    return out
+                                                _ptr(out), 1 if dtype == torch.complex128 else 0, _ptr(lo),
+                                                _stream()))
+    return (out, lo) if with_lo else out
+
+
+def transfer_pair(method: str, n: int, m: int, ps, z: float, energy: float):
+    """(H_hi, H_lo) complex64 pair of the Fresnel ('fresnel') or angular-spectrum
+    ('as') transfer function, evaluated in float64 on the device."""
+    kind = _lib.WAP_TF_ANGULAR if method == "as" else _lib.WAP_TF_FRESNEL
+    return _transfer(kind, n, m, ps, z, energy, torch.complex64, with_lo=True)
 
 
 def fresnel_propagation_kernel(n: int, m: int, ps, z: float, energy: float, *, dtype=torch.complex128):
@@ -279,7 +306,7 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     V, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(potential, probe, positions, draw, dev)
     if N < 1:
         raise ValueError("need at least one array to stack")  # jnp.stack([]) in the reference
-    H = _to(prop_kernel, torch.complex64, dev)
+    H, H_lo = split_transfer(prop_kernel, dev)
     if H.shape != (ny, nx):
         raise ValueError(f"prop_kernel shape {tuple(H.shape)} does not match grid {(ny, nx)}")
     plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
@@ -288,7 +315,7 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
-        _ptr(pos), _ptr(H), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
+        _ptr(pos), _ptr(H), _ptr(H_lo), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
         _ptr(stack), _stream()))
     if not batched:
         exit_wave, dp = exit_wave[0], dp[0]

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .propagation import _ptr, _stream, angular_spectrum_propagation_kernel, fresnel_propagation_kernel, get_plan
+from .propagation import _ptr, _stream, get_plan, transfer_pair
 
 
 @dataclass
@@ -37,7 +37,8 @@ class DeviceClass:
     probe: torch.Tensor       # (ny, nx) complex64
     positions: torch.Tensor   # (B, 2) int32
     draw: torch.Tensor        # (B,) int32
-    H: torch.Tensor           # (ny, nx) complex64
+    H: torch.Tensor           # (ny, nx) complex64 (hi part)
+    H_lo: torch.Tensor        # (ny, nx) complex64 rounding remainder
     exit: torch.Tensor        # (B, ny, nx) complex64 (working buffer)
     dp: torch.Tensor          # (B, ny, nx) float32
 
@@ -60,9 +61,8 @@ def to_device_class(w, device=None) -> DeviceClass:
                           dtype=torch.int32).to(dev).contiguous()
     draw = torch.as_tensor(w.draw_of_probe if w.draw_of_probe is not None else np.zeros(B, np.int32),
                            dtype=torch.int32).to(dev).contiguous()
-    tf = angular_spectrum_propagation_kernel if w.method == "as" else fresnel_propagation_kernel
-    H = tf(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy, dtype=torch.complex64)
-    return DeviceClass(w.ny, w.nx, w.n_slices, V.shape[0], B, w.dz, w.energy, V, probe, pos, draw, H,
+    H, H_lo = transfer_pair(w.method, w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    return DeviceClass(w.ny, w.nx, w.n_slices, V.shape[0], B, w.dz, w.energy, V, probe, pos, draw, H, H_lo,
                        torch.empty((B, w.ny, w.nx), dtype=torch.complex64, device=dev),
                        torch.empty((B, w.ny, w.nx), dtype=torch.float32, device=dev))
 
@@ -75,7 +75,7 @@ def _fwd(c: DeviceClass, b0: int, nb: int) -> None:
     pos = ctypes.c_void_p(c.positions.data_ptr() + b0 * 8)
     dr = ctypes.c_void_p(c.draw.data_ptr() + b0 * 4)
     _lib.check(_lib.lib().wap_multislice_fwd(
-        plan.handle, _ptr(c.V), c.n_slices, c.n_draws, dr, _ptr(c.probe), nb, 0, pos, _ptr(c.H),
+        plan.handle, _ptr(c.V), c.n_slices, c.n_draws, dr, _ptr(c.probe), nb, 0, pos, _ptr(c.H), _ptr(c.H_lo),
         c.dz, c.energy, ex, dp, None, _stream()))
 
 
