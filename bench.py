@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--impl", default="wap", choices=["wap", "reference"])
     ap.add_argument("--small", action="store_true", help="tiny workload (testing the harness)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/grad/err/cpu sections")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="reduced scan for ncu captures: 512 probes 256^2 x 4 slices + 32 probes 512^2 x 4 "
+                         "slices (waves 256 + 64 MB, above L2), one warm-up and one step, no extras")
     return ap.parse_args()
 
 
@@ -157,7 +160,11 @@ def main():
     args = parse()
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
-    classes_host = S.batched_scan(0, small=args.small)
+    if args.profile_case:
+        classes_host = [S.batched_scan_class(0, 256, 4, 16, 2), S.batched_scan_class(1, 512, 4, 4, 2)]
+        args.steps, args.warmup, args.no_extras = 1, 1, True
+    else:
+        classes_host = S.batched_scan(0, small=args.small)
 
     if args.impl == "reference":
         run_reference(args, classes_host, rank)

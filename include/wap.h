@@ -136,6 +136,7 @@ int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws
 #define WAP_KIND_WPM_ROW 3    /* WPM row pass (K row IFFTs + blend) */
 #define WAP_KIND_WPM_BINS 4   /* WPM per-slice bin edges */
 #define WAP_KIND_SCHED 5      /* persistent batched scheduler */
+#define WAP_KIND_TRANS 6      /* transmission table exp(i phi(V)) */
 /* Number of kernels this library has launched in this process (all kinds). */
 long long wap_launch_count(void);
 int wap_profile_enable(int on);

@@ -47,9 +47,10 @@ SIGNATURES = {
     "wap_profile_read": (_I, [_I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
 }
 
-KIND_ROW, KIND_COL, KIND_WPM_COL, KIND_WPM_ROW, KIND_WPM_BINS, KIND_SCHED = range(6)
+KIND_ROW, KIND_COL, KIND_WPM_COL, KIND_WPM_ROW, KIND_WPM_BINS, KIND_SCHED, KIND_TRANS = range(7)
 KIND_NAMES = {KIND_ROW: "row_pass_kernel", KIND_COL: "col_pass_kernel", KIND_WPM_COL: "wpm_col_kernel",
-              KIND_WPM_ROW: "wpm_row_kernel", KIND_WPM_BINS: "wpm_bins_kernel", KIND_SCHED: "scan_persistent_kernel"}
+              KIND_WPM_ROW: "wpm_row_kernel", KIND_WPM_BINS: "wpm_bins_kernel", KIND_SCHED: "scan_persistent_kernel",
+              KIND_TRANS: "trans_table_kernel"}
 
 _lib = None
 _lock = threading.Lock()

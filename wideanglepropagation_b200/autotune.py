@@ -68,3 +68,78 @@ def candidates(ny, nx):
                     continue
                 out.append((row_e, col_e, col_w))
     return out
+
+
+def _time_config(plan, run, reps=3):
+    import torch
+    run()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(reps):
+        s.record()
+        run()
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    return best
+
+
+def tune(ny: int, nx: int, op: int = 0, n_bins: int = 0, batch: int | None = None, n_slices: int = 6,
+         verbose: bool = False):
+    """Time every candidate launch shape on a synthetic multislice of ``batch``
+    probes and cache the fastest; returns (config, {config: ms})."""
+    import numpy as np
+    import torch
+    from . import _lib
+    from .propagation import get_plan, simulate_fresnel_as, simulate_wpm
+    if batch is None:
+        batch = max(1, (64 * 2 ** 20) // (ny * nx * 8)) if op == 0 else 1
+    rng = np.random.default_rng(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    V = torch.as_tensor(rng.uniform(0, 30, (n_slices, ny, nx)).astype(np.float32), device=dev)
+    probe = torch.ones((ny, nx), dtype=torch.complex64, device=dev)
+    pos = torch.as_tensor(np.stack([rng.integers(0, ny, batch), rng.integers(0, nx, batch)], 1).astype(np.int32),
+                          device=dev)
+    H = torch.exp(1j * torch.as_tensor(rng.uniform(-3, 3, (ny, nx)), device=dev)).to(torch.complex128)
+    plan = get_plan(ny, nx, batch, op, n_bins)
+    old = plan.config()
+
+    def run():
+        if op == _lib.WAP_OP_WPM:
+            simulate_wpm(V, probe, 2.0, 300e3, (0.05, 0.05), n_bins, 1.0, return_wavefronts=False, positions=pos)
+        else:
+            simulate_fresnel_as(V, probe, H, 2.0, 300e3, return_wavefronts=False, positions=pos)
+
+    times = {}
+    for cfg in candidates(ny, nx):
+        try:
+            plan.set_config(*cfg)
+        except ValueError:
+            continue
+        times[cfg] = _time_config(plan, run)
+        if verbose:
+            print(f"  {ny}x{nx} op{op} {cfg}: {times[cfg]:.3f} ms", flush=True)
+    best = min(times, key=times.get)
+    plan.set_config(*best) if best else plan.set_config(*old)
+    store(ny, nx, op, n_bins, best)
+    return best, times
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser(description="autotune the multislice launch shapes on this GPU")
+    ap.add_argument("--grids", default="256,512,1024", help="comma-separated square grid sizes")
+    ap.add_argument("--wpm-bins", default="16", help="comma-separated WPM bin counts to tune (empty: none)")
+    args = ap.parse_args(argv)
+    for n in [int(v) for v in args.grids.split(",") if v]:
+        best, _ = tune(n, n, 0, 0, verbose=True)
+        print(f"{n}x{n} fresnel/as best {best}", flush=True)
+        for k in [int(v) for v in args.wpm_bins.split(",") if v]:
+            best, _ = tune(n, n, 1, k, verbose=True)
+            print(f"{n}x{n} wpm K={k} best {best}", flush=True)
+    print(f"cache: {CACHE_PATH}")
+
+
+if __name__ == "__main__":
+    main()

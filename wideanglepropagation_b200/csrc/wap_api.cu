@@ -317,6 +317,7 @@ int wap_plan_destroy(wap_plan* p) {
   cudaFree(p->ky2);
   cudaFree(p->kx2);
   cudaFree(p->refs);
+  cudaFree(p->ttab);
   delete p;
   return WAP_OK;
 }
@@ -414,6 +415,7 @@ ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo) {
 static double row_bytes(const wap_plan* p, const RowArgs& r, int n_probes) {
   double per = 16;
   if (r.flags & (ROW_TRANS | ROW_ADJOINT)) per += 4;
+  if (r.flags & ROW_TRANS_TAB) per += 8;
   if (r.snap) per += 8;
   if (r.flags & ROW_ADJOINT) per += 16;
   return per * (double)p->ny * p->nx * n_probes;
@@ -472,6 +474,33 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   r.src = reinterpret_cast<const float2*>(psi0);
   r.src_bstride = psi0_per_probe ? plane : 0;
   r.shifts = positions;
+  // When several probes see each potential slice, tabulate exp(i phi(V)) once
+  // per (draw, slice) instead of evaluating it per probe.
+  int trans_flag = ROW_TRANS;
+  if (n_probes >= 2 * n_draws) {
+    const size_t need = (size_t)n_draws * n_slices * plane;
+    cudaError_t e = cudaSuccess;
+    if (need > p->ttab_cap) {
+      cudaFree(p->ttab);
+      p->ttab = nullptr;
+      p->ttab_cap = 0;
+      e = cudaMalloc(&p->ttab, need * sizeof(float2));
+      if (e == cudaSuccess) p->ttab_cap = need;
+    }
+    if (e == cudaSuccess) {
+      const long long n4 = (long long)need / 4;
+      const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
+      count_launch();
+      trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
+          V, p->ttab, n4, r.ri_a, r.ri_inv_den, r.kphase);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
+      prof_end(tok, st, 12.0 * (double)need);
+      r.ttab = p->ttab;
+      trans_flag = ROW_TRANS_TAB;
+    } else {
+      cudaGetLastError();  // workspace unavailable: evaluate t per probe
+    }
+  }
   ColArgs c = base_col_args(p, H, H_lo);
   c.psi = r.psi;
   c.psi_bstride = plane;
@@ -479,7 +508,7 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
 
   for (int s = 0; s <= n_slices; ++s) {
     r.slice = s;
-    r.flags = (s == 0 ? ROW_LOAD_SRC : ROW_IFFT) | (s < n_slices ? (ROW_TRANS | ROW_FFT) : 0);
+    r.flags = (s == 0 ? ROW_LOAD_SRC : ROW_IFFT) | (s < n_slices ? (trans_flag | ROW_FFT) : 0);
     r.snap = nullptr;
     if (stack && s >= 1) {
       r.snap = reinterpret_cast<float2*>(stack) + (long long)(s - 1) * plane;

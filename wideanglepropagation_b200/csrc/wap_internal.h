@@ -23,6 +23,8 @@ struct wap_plan {
   double hvac_key[4] = {0, 0, 0, 0};        // (dy, dx, dz, energy) of hvac
   float* refs = nullptr;                    // (draws, n_slices, n_bins)
   size_t refs_cap = 0;
+  float2* ttab = nullptr;                   // transmission table (draws, n_slices, ny, nx)
+  size_t ttab_cap = 0;
 };
 
 namespace wap {

@@ -41,6 +41,7 @@ enum RowFlags : int {
   ROW_FFT = 8,        // forward row FFT last
   ROW_ADJOINT = 16,   // adjoint: gradient accumulation + conj(t)
   ROW_SCALE_SRC = 32, // multiply the loaded source by src_scale (adjoint seed)
+  ROW_TRANS_TAB = 64, // multiply by the precomputed transmission table ttab
 };
 
 enum ColFlags : int {
@@ -65,6 +66,7 @@ struct RowArgs {
   const float2* aux;         // ROW_ADJOINT: forward wave psi_s entering slice s
   long long aux_bstride;
   float* grad;               // ROW_ADJOINT: dL/dV, laid out like V, accumulated
+  const float2* ttab;        // ROW_TRANS_TAB: exp(i phi(V)) laid out like V
   int ny, nx;
   int slice;
   int flags;
@@ -113,6 +115,20 @@ __device__ __forceinline__ float2 transmission(float v, float a, float inv_den, 
   float s, c;
   sincosf(kphase * refr_minus_one(v, a, inv_den), &s, &c);
   return make_float2(c, s);
+}
+
+// transmission table: ttab[i] = t(V[i]) for every draw and slice, computed
+// once and shared by all probes that see the same potential
+static __global__ void __launch_bounds__(256) trans_table_kernel(const float* __restrict__ V, float2* __restrict__ ttab,
+                                                          long long n4, float a, float inv_den, float kphase) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(V) + i);
+    const float2 t0 = transmission(v.x, a, inv_den, kphase), t1 = transmission(v.y, a, inv_den, kphase);
+    const float2 t2 = transmission(v.z, a, inv_den, kphase), t3 = transmission(v.w, a, inv_den, kphase);
+    float4* o = reinterpret_cast<float4*>(ttab) + 2 * i;
+    o[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
+    o[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -184,7 +200,12 @@ row_pass_kernel(const RowArgs a) {
     for (int e = 0; e < E; ++e) __stcs(sp + t + T * e, v[e]);
   }
 
-  if (f & (ROW_TRANS | ROW_ADJOINT)) {
+  if (f & ROW_TRANS_TAB) {
+    const int d = a.draw ? a.draw[b] : 0;
+    const float2* trow = a.ttab + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
+  } else if (f & (ROW_TRANS | ROW_ADJOINT)) {
     const int d = a.draw ? a.draw[b] : 0;
     const float* vrow = a.V + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
     if (f & ROW_ADJOINT) {
