@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--impl", default="wap", choices=["wap", "reference"])
     ap.add_argument("--small", action="store_true", help="tiny workload (testing the harness)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/grad/err/cpu sections")
+    ap.add_argument("--mode", default="persistent", choices=["persistent", "batched", "graph"],
+                    help="batched execution mode timed as the headline")
     ap.add_argument("--profile-case", action="store_true",
                     help="reduced scan for ncu captures: 512 probes 256^2 x 4 slices + 32 probes 512^2 x 4 "
                          "slices (waves 256 + 64 MB, above L2), one warm-up and one step, no extras")
@@ -196,7 +198,7 @@ def main():
     _lib.lib()
     launches0 = _lib.launch_count()
     classes = [to_device_class(w, dev) for w in classes_host]
-    scan = BatchedScan(classes, mode="batched")
+    scan = BatchedScan(classes, mode=args.mode)
     total_ss = scan.slice_steps()
 
     # --- headline: batched, inputs resident in HBM --------------------------
@@ -215,18 +217,20 @@ def main():
     torch.cuda.synchronize()
     l1 = _lib.launch_count()
     clk = clocks.stop()
+    # graph replays bypass the library's host-side counter: count the nodes
+    graph_launches = scan.launches() * args.steps if args.mode in ("graph", "persistent") else 0
     barrier()
     ms = max_over_ranks(start.elapsed_time(stop))
     ms_per_step = ms / args.steps
     value = total_ss * world / (ms_per_step / 1e3)
-    gpu_launches = l1 - l0
+    gpu_launches = (l1 - l0) + graph_launches
 
     extras = {}
     # --- roofline: per-pass device time with the library's event tracing -----
     _lib.profile_reset()
     _lib.profile_enable(True)
     for _ in range(max(1, min(args.steps, 3))):
-        scan.step()
+        scan._eager()      # eager launches so that the tracer records them
     torch.cuda.synchronize()
     _lib.profile_enable(False)
     kinds = {}
@@ -249,8 +253,13 @@ def main():
                 "launches": n, "avg_launch_us": 1e3 * kms / n,
                 "share": {k: v[1] / sum(x[1] for x in kinds.values()) for k, v in kinds.items()}}
 
+    if scan.sched is not None:
+        st = scan.sched.status()
+        if st != 0:
+            raise RuntimeError(f"persistent scan reported status {st}")
     if not args.no_extras and rank == 0:
         extras.update(_plain(classes, args))
+        extras.update(_per_pass(classes, args))
         extras.update(_grad_ratio(args))
         extras.update(_err_vs_fp64(classes, classes_host))
 
@@ -269,7 +278,11 @@ def main():
                 "config": {"workload": WORKLOAD, "slice_steps_per_step": total_ss,
                            "pixel_slice_steps_per_step": sum(c.pixel_slice_steps for c in classes),
                            "l2": "inputs larger than L2 (potential 241 MB, waves 640 MB per step)",
-                           "mode": "batched per-pass launches", "parallelism": f"probe shards x{world}"},
+                           "mode": {"persistent": "one persistent kernel per step (device ticket queue, TMA tiles), "
+                                                  "CUDA-graph replay",
+                                    "batched": "per-pass launches over all probes of a class",
+                                    "graph": "per-pass launches, CUDA-graph replay"}[args.mode],
+                           "parallelism": f"probe shards x{world}"},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clk,
                 "cpu_baseline": cpu}
         line.update(extras)
@@ -323,6 +336,23 @@ def _plain(classes, args):
     return {"plain": {"value": rate, "unit": "slice-steps/s", "sample": "16 probes per class, one probe per launch"},
             "per_class_slice_steps_per_s": {f"{c.ny}x{c.nx}": {"batched": 1 / b, "plain": 1 / p}
                                             for c, b, p in zip(classes, bper, per)}}
+
+
+def _per_pass(classes, args):
+    import torch
+    from wideanglepropagation_b200.scan import BatchedScan
+    sc = BatchedScan(classes, mode="batched")
+    sc.step()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(2):
+        sc.step()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / 2
+    return {"batched_per_pass": {"value": sc.slice_steps() / (ms / 1e3), "unit": "slice-steps/s",
+                                 "ms_per_step": ms}}
 
 
 def _grad_ratio(args):

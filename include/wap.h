@@ -125,6 +125,51 @@ int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws
                        const float* grad_dp, const float* grad_exit, float* grad_V,
                        float* work, void* stream);
 
+/* Batched scan: one grid class of probes (square n x n grid, n in
+ * {128, 256, 512, 1024}) with its own potential draws, probe and propagator.
+ * All pointers are device pointers; the probe is shared and rolled to each
+ * position like move_probe (propagation.py:263-276). */
+typedef struct wap_scan_class {
+  int n, n_slices, n_draws, n_probes;
+  const float* V;            /* (n_draws, n_slices, n, n) float32 volts */
+  const int32_t* draw;       /* (n_probes) or NULL */
+  const float* psi0;         /* (n, n) complex64 probe */
+  const int32_t* positions;  /* (n_probes, 2) probe centres or NULL */
+  const float* H;            /* (n, n) complex64 transfer function */
+  const float* H_lo;         /* (n, n) complex64 remainder or NULL */
+  double dz, energy;
+  float* exit;               /* (n_probes, n, n) complex64: working buffer, exit waves */
+  float* dp;                 /* (n_probes, n, n) float32 or NULL */
+  int group;                 /* probes advanced together (0: automatic) */
+} wap_scan_class;
+
+typedef struct wap_scan wap_scan;
+
+/* Persistent batched scheduler for simulate_fresnel_as over many probes
+ * (the caller loop of propagation.py:305-352 over move_probe positions).
+ * wap_scan_create lays out the device work queue (groups of probes x passes
+ * x tiles), tensor maps and transmission tables for up to 4 classes;
+ * wap_scan_run issues, on `stream`, the counter resets, one transmission
+ * table kernel per class and ONE persistent kernel that runs every tile of
+ * every class (capturable in a CUDA graph).  Every device-side wait is
+ * bounded; wap_scan_status (synchronising) returns WAP_ERR_TIMEOUT if one
+ * expired. */
+int wap_scan_create(wap_scan** scan, int n_classes, const wap_scan_class* classes);
+int wap_scan_run(wap_scan* scan, void* stream);
+int wap_scan_status(wap_scan* scan, int* status);
+int wap_scan_info(const wap_scan* scan, long long* tickets, int* grid, int* group0);
+int wap_scan_destroy(wap_scan* scan);
+/* Failure injection for tests (no counterpart in the reference): tiles of
+ * pass `pass` get a dependency nothing satisfies, so their bounded waits
+ * expire after `spin_limit` polls and the run reports WAP_ERR_TIMEOUT; pass
+ * -1 restores normal operation.  No device fault is involved. */
+int wap_scan_debug_stall(wap_scan* scan, int pass, long long spin_limit);
+/* Debug validation (no counterpart in the reference): with on != 0 every
+ * task is range-checked before use and a bad one is skipped; record (6 ints,
+ * nullable) receives [where, class, pass, probe, tile, valid] of the first
+ * violation (where = 0: none). */
+int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
+
 /* Kernel-level tracing (no counterpart in the reference, which has none).
  * While enabled, each pass launch is bracketed by CUDA events on its stream
  * and tagged with its kind and algorithmic bytes (wave in/out, potential,

@@ -1,0 +1,115 @@
+"""Persistent batched scheduler (wap_scan_*): same results as the per-pass
+path and the FP64 oracle, CUDA-graph replay, and bounded waits that report
+a timeout instead of hanging (failure injected from the host)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def wap():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import wideanglepropagation_b200 as w
+    return w
+
+
+def _classes(wap, spec, seed=0):
+    from wideanglepropagation_b200.scan import to_device_class
+    S = wap.synthetic
+    return [to_device_class(S.batched_scan_class(seed + i, n, ns, side, draws)) for i, (n, ns, side, draws) in enumerate(spec)]
+
+
+def _run(wap, classes, mode, groups=None):
+    from wideanglepropagation_b200.scan import BatchedScan
+    sc = BatchedScan(classes, mode=mode, groups=groups)
+    sc.step()
+    torch.cuda.synchronize()
+    if sc.sched is not None:
+        assert sc.sched.status() == 0
+    return [c.exit.clone() for c in classes], [c.dp.clone() for c in classes], sc
+
+
+def rel(a, b):
+    a = a.double() if not a.is_complex() else a.to(torch.complex128)
+    b = b.double() if not b.is_complex() else b.to(torch.complex128)
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+@pytest.mark.parametrize("spec", [
+    [(128, 5, 4, 2), (256, 4, 2, 1)],          # uneven: two sizes, draws
+    [(512, 3, 2, 1)],
+    [(1024, 2, 1, 2)],
+    [(256, 6, 3, 1), (128, 3, 2, 1), (512, 2, 1, 1)],
+])
+def test_persistent_matches_per_pass(wap, spec):
+    classes = _classes(wap, spec)
+    ex_b, dp_b, _ = _run(wap, classes, "batched")
+    ex_p, dp_p, _ = _run(wap, classes, "persistent")
+    for a, b in zip(ex_p, ex_b):
+        assert rel(a, b) < 1e-7
+    for a, b in zip(dp_p, dp_b):
+        assert rel(a, b) < 1e-7
+
+
+def test_persistent_vs_oracle_and_groups(wap):
+    from oracle import propagation_oracle as O
+    spec = [(256, 6, 3, 2), (128, 4, 2, 1)]
+    classes = _classes(wap, spec, seed=3)
+    host = [wap.synthetic.batched_scan_class(3 + i, *s) for i, s in enumerate(spec)]
+    ex, dp, _ = _run(wap, classes, "persistent", groups=[5, 3])   # groups that do not divide B
+    for c, w, e, d in zip(classes, host, ex, dp):
+        H = O.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+        for b in (0, c.n_probes // 2, c.n_probes - 1):
+            p0 = O.move_probe(w.probe, tuple(w.positions[b]))
+            rex, rdp, _ = O.simulate_fresnel_as(w.potential[w.draw_of_probe[b]], p0, H, w.dz, w.energy,
+                                                return_wavefronts=False)
+            assert O.rel_l2(e[b].cpu().numpy(), rex) < 1e-5
+            assert O.rel_l2(d[b].cpu().numpy(), rdp) < 1e-5
+
+
+def test_graph_replay_is_repeatable(wap):
+    from wideanglepropagation_b200.scan import BatchedScan
+    classes = _classes(wap, [(256, 4, 4, 1), (512, 2, 2, 1)])
+    sc = BatchedScan(classes, mode="persistent")
+    sc.capture()
+    sc.graph.replay()
+    torch.cuda.synchronize()
+    first = [c.dp.clone() for c in classes]
+    for c in classes:
+        c.dp.zero_()
+    sc.graph.replay()
+    torch.cuda.synchronize()
+    assert sc.sched.status() == 0
+    for a, c in zip(first, classes):
+        assert torch.equal(a, c.dp)
+
+
+def test_bounded_wait_reports_timeout(wap):
+    """A dependency that nothing satisfies (set from the host) makes the
+    bounded waits expire: the run returns WAP_ERR_TIMEOUT and the context stays
+    usable for the next, normal run."""
+    from wideanglepropagation_b200 import _lib
+    from wideanglepropagation_b200.scan import BatchedScan
+    classes = _classes(wap, [(128, 3, 2, 1)])
+    ref_ex, _, _ = _run(wap, classes, "batched")
+    sc = BatchedScan(classes, mode="persistent")
+    sc.sched.debug_stall(1, 1 << 12)
+    sc.sched.run()
+    torch.cuda.synchronize()
+    assert sc.sched.status() == _lib.WAP_ERR_TIMEOUT
+    sc.sched.debug_stall(-1, 0)
+    sc.sched.run()
+    torch.cuda.synchronize()
+    assert sc.sched.status() == 0
+    assert rel(classes[0].exit, ref_ex[0]) < 1e-7
+
+
+def test_scan_rejects_unsupported(wap):
+    from wideanglepropagation_b200.scan import PersistentScan
+    classes = _classes(wap, [(128, 2, 1, 1)])
+    classes[0].ny = classes[0].nx = 64
+    with pytest.raises(ValueError, match="128, 256, 512 or 1024"):
+        PersistentScan(classes)

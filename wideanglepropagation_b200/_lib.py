@@ -41,6 +41,13 @@ SIGNATURES = {
     "wap_wpm_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P]),
     "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
     "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "wap_scan_create": (_I, [ctypes.POINTER(_P), _I, _P]),
+    "wap_scan_run": (_I, [_P, _P]),
+    "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
+    "wap_scan_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "wap_scan_destroy": (_I, [_P]),
+    "wap_scan_debug_stall": (_I, [_P, _I, ctypes.c_longlong]),
+    "wap_scan_debug_checks": (_I, [_P, _I, _P]),
     "wap_launch_count": (ctypes.c_longlong, []),
     "wap_profile_enable": (_I, [_I]),
     "wap_profile_reset": (_I, []),
@@ -51,6 +58,13 @@ KIND_ROW, KIND_COL, KIND_WPM_COL, KIND_WPM_ROW, KIND_WPM_BINS, KIND_SCHED, KIND_
 KIND_NAMES = {KIND_ROW: "row_pass_kernel", KIND_COL: "col_pass_kernel", KIND_WPM_COL: "wpm_col_kernel",
               KIND_WPM_ROW: "wpm_row_kernel", KIND_WPM_BINS: "wpm_bins_kernel", KIND_SCHED: "scan_persistent_kernel",
               KIND_TRANS: "trans_table_kernel"}
+
+class ScanClass(ctypes.Structure):
+    """Mirror of ``wap_scan_class`` (include/wap.h)."""
+    _fields_ = [("n", _I), ("n_slices", _I), ("n_draws", _I), ("n_probes", _I),
+                ("V", _P), ("draw", _P), ("psi0", _P), ("positions", _P), ("H", _P), ("H_lo", _P),
+                ("dz", _D), ("energy", _D), ("exit", _P), ("dp", _P), ("group", _I)]
+
 
 _lib = None
 _lock = threading.Lock()

@@ -250,28 +250,41 @@ __device__ __forceinline__ void dft(float2 (&a)[R]) {
 // ----------------------------------------------------------------------------
 // shared-memory exchange policies
 // ----------------------------------------------------------------------------
+// Block-level barrier: __syncthreads, or named barrier BAR over NT threads
+// when only part of the block (e.g. the compute warps of a warp-specialised
+// kernel) takes part in the transform.
+template <int BAR, int NT>
+__device__ __forceinline__ void block_sync() {
+  if constexpr (BAR == 0) {
+    __syncthreads();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(NT) : "memory");
+  }
+}
+
 // One transform per row segment of shared memory; index p padded by one word
 // per 16 so that radix-R Stockham scatters are bank-conflict free.
-template <bool WARP_LOCAL>
+template <bool WARP_LOCAL, int BAR = 0, int NT = 0>
 struct RowExchange {
   float2* base;
   __device__ __forceinline__ void st(int p, float2 v) const { base[p + (p >> 4)] = v; }
   __device__ __forceinline__ float2 ld(int p) const { return base[p + (p >> 4)]; }
   __device__ __forceinline__ void sync() const {
     if constexpr (WARP_LOCAL) __syncwarp();
-    else __syncthreads();
+    else block_sync<BAR, NT>();
   }
   __host__ __device__ static constexpr int padded(int n) { return n + (n >> 4); }
 };
 
 // One transform per column of a row-major [N][W] tile (lanes run along the
 // columns, so stores of one Stockham position by a warp are contiguous).
+template <int BAR = 0, int NT = 0>
 struct ColExchange {
   float2* base;
   int w, c;
   __device__ __forceinline__ void st(int p, float2 v) const { base[p * w + c] = v; }
   __device__ __forceinline__ float2 ld(int p) const { return base[p * w + c]; }
-  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ void sync() const { block_sync<BAR, NT>(); }
 };
 
 // ----------------------------------------------------------------------------

@@ -293,7 +293,7 @@ col_pass_kernel(const ColArgs a) {
   const int nx = a.nx;
   const long long plane = (long long)NY * nx;
   float2* ptile = a.psi + (long long)b * a.psi_bstride + (long long)blockIdx.x * W;
-  const ColExchange xs{tile, W, c};
+  const ColExchange<> xs{tile, W, c};
   const int f = a.flags;
 
   float2 v[E];
@@ -483,7 +483,7 @@ wpm_col_kernel(const WpmColArgs a) {
   __syncthreads();
   const int nx = a.nx;
   const long long plane = (long long)NY * nx;
-  const ColExchange xs{tile, W, c};
+  const ColExchange<> xs{tile, W, c};
 
   float2 v[E];
   tile_load<NY>(tile, a.psi + (long long)b * plane + (long long)blockIdx.x * W, W, nx);

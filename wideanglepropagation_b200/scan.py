@@ -7,9 +7,12 @@ loop of ``simulate_fresnel_as(V, move_probe(probe, pos), H, dz, E)``
 (propagation.py:263-276, :305-352); here every probe of every class is
 advanced in the same kernels.  Three execution modes are offered:
 
-``plain``      one probe per launch sequence (the reference's loop, on the GPU)
-``batched``    per class, every pass covers all probes of the class
-``graph``      ``batched`` captured once into a CUDA graph and replayed
+``plain``       one probe per launch sequence (the reference's loop, on the GPU)
+``batched``     per class, every pass covers all probes of the class
+``graph``       ``batched`` captured once into a CUDA graph and replayed
+``persistent``  every class in ONE persistent kernel (``wap_scan_run``: device
+                ticket queue, L2-resident probe groups, TMA tile loads),
+                captured once into a CUDA graph and replayed
 """
 from __future__ import annotations
 
@@ -87,20 +90,72 @@ def launches_per_step(classes: List[DeviceClass], mode: str) -> int:
     return sum(p * ((c.n_probes + 65534) // 65535) for p, c in zip(per, classes))
 
 
-class BatchedScan:
-    """Runs a list of ``DeviceClass`` scans in one of the three modes."""
+class PersistentScan:
+    """Owns a ``wap_scan`` (device work queue over all classes)."""
 
-    def __init__(self, classes: List[DeviceClass], mode: str = "batched", plain_subset: Optional[int] = None):
-        if mode not in ("plain", "batched", "graph"):
+    def __init__(self, classes: List[DeviceClass], groups: Optional[List[int]] = None):
+        arr = (_lib.ScanClass * len(classes))()
+        for i, c in enumerate(classes):
+            if c.ny != c.nx:
+                raise ValueError("the persistent scheduler takes square grids")
+            arr[i] = _lib.ScanClass(c.ny, c.n_slices, c.n_draws, c.n_probes, c.V.data_ptr(), c.draw.data_ptr(),
+                                    c.probe.data_ptr(), c.positions.data_ptr(), c.H.data_ptr(),
+                                    c.H_lo.data_ptr() if c.H_lo is not None else None, c.dz, c.energy,
+                                    c.exit.data_ptr(), c.dp.data_ptr(), (groups or [0] * len(classes))[i])
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().wap_scan_create(ctypes.byref(h), len(classes), ctypes.cast(arr, ctypes.c_void_p)))
+        self.handle = h
+        self.classes = classes   # keeps the buffers alive
+
+    def run(self) -> None:
+        _lib.check(_lib.lib().wap_scan_run(self.handle, _stream()))
+
+    def status(self) -> int:
+        st = ctypes.c_int()
+        rc = _lib.lib().wap_scan_status(self.handle, ctypes.byref(st))
+        if rc not in (0, _lib.WAP_ERR_TIMEOUT):
+            _lib.check(rc)
+        return st.value
+
+    def info(self) -> dict:
+        t, g, g0 = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().wap_scan_info(self.handle, ctypes.byref(t), ctypes.byref(g), ctypes.byref(g0)))
+        return {"tickets": t.value, "grid": g.value}
+
+    def debug_stall(self, pass_index: int, spin_limit: int = 0) -> None:
+        _lib.check(_lib.lib().wap_scan_debug_stall(self.handle, int(pass_index), int(spin_limit)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.lib().wap_scan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchedScan:
+    """Runs a list of ``DeviceClass`` scans in one of the four modes."""
+
+    def __init__(self, classes: List[DeviceClass], mode: str = "batched", plain_subset: Optional[int] = None,
+                 groups: Optional[List[int]] = None):
+        if mode not in ("plain", "batched", "graph", "persistent"):
             raise ValueError(f"unknown mode {mode!r}")
         self.classes = classes
         self.mode = mode
         self.plain_subset = plain_subset
         self.graph = None
+        self.sched = PersistentScan(classes, groups) if mode == "persistent" else None
         for c in classes:   # create plans outside any capture
             get_plan(c.ny, c.nx, c.n_probes, _lib.WAP_OP_FRESNEL_AS)
 
     def _eager(self):
+        if self.sched is not None:
+            self.sched.run()
+            return
         for c in self.classes:
             if self.mode == "plain":
                 n = c.n_probes if self.plain_subset is None else min(self.plain_subset, c.n_probes)
@@ -121,7 +176,7 @@ class BatchedScan:
             self._eager()
 
     def step(self) -> None:
-        if self.mode == "graph":
+        if self.mode in ("graph", "persistent"):
             if self.graph is None:
                 self.capture()
             self.graph.replay()
@@ -134,6 +189,8 @@ class BatchedScan:
         return sum(c.slice_steps for c in self.classes)
 
     def launches(self) -> int:
+        if self.mode == "persistent":
+            return len(self.classes) + 1
         if self.mode == "plain" and self.plain_subset is not None:
             return sum((2 * c.n_slices + 1) * min(self.plain_subset, c.n_probes) for c in self.classes)
         return launches_per_step(self.classes, "plain" if self.mode == "plain" else "batched")
