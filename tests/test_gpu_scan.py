@@ -45,13 +45,16 @@ def rel(a, b):
     [(256, 6, 3, 1), (128, 3, 2, 1), (512, 2, 1, 1)],
 ])
 def test_persistent_matches_per_pass(wap, spec):
+    """Same math as the per-pass kernels; the scheduler may use a different
+    radix plan (elements per thread), so results agree to float32 FFT
+    rounding (2e-6), not bit for bit."""
     classes = _classes(wap, spec)
     ex_b, dp_b, _ = _run(wap, classes, "batched")
     ex_p, dp_p, _ = _run(wap, classes, "persistent")
     for a, b in zip(ex_p, ex_b):
-        assert rel(a, b) < 1e-7
+        assert rel(a, b) < 2e-6
     for a, b in zip(dp_p, dp_b):
-        assert rel(a, b) < 1e-7
+        assert rel(a, b) < 2e-6
 
 
 def test_persistent_vs_oracle_and_groups(wap):
@@ -104,7 +107,7 @@ def test_bounded_wait_reports_timeout(wap):
     sc.sched.run()
     torch.cuda.synchronize()
     assert sc.sched.status() == 0
-    assert rel(classes[0].exit, ref_ex[0]) < 1e-7
+    assert rel(classes[0].exit, ref_ex[0]) < 2e-6
 
 
 def test_scan_rejects_unsupported(wap):

@@ -119,15 +119,32 @@ __device__ __forceinline__ float2 transmission(float v, float a, float inv_den, 
 
 // transmission table: ttab[i] = t(V[i]) for every draw and slice, computed
 // once and shared by all probes that see the same potential
+// ttab[i] = t(V[i]) * post_scale; post_scale is a power of two (exact), used
+// to fold the 1/(ny nx) of the inverse transform into the table
 static __global__ void __launch_bounds__(256) trans_table_kernel(const float* __restrict__ V, float2* __restrict__ ttab,
-                                                          long long n4, float a, float inv_den, float kphase) {
+                                                          long long n4, float a, float inv_den, float kphase,
+                                                          float post_scale = 1.0f) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(V) + i);
-    const float2 t0 = transmission(v.x, a, inv_den, kphase), t1 = transmission(v.y, a, inv_den, kphase);
-    const float2 t2 = transmission(v.z, a, inv_den, kphase), t3 = transmission(v.w, a, inv_den, kphase);
+    const float2 t0 = cscale(transmission(v.x, a, inv_den, kphase), post_scale);
+    const float2 t1 = cscale(transmission(v.y, a, inv_den, kphase), post_scale);
+    const float2 t2 = cscale(transmission(v.z, a, inv_den, kphase), post_scale);
+    const float2 t3 = cscale(transmission(v.w, a, inv_den, kphase), post_scale);
     float4* o = reinterpret_cast<float4*>(ttab) + 2 * i;
     o[0] = make_float4(t0.x, t0.y, t1.x, t1.y);
     o[1] = make_float4(t2.x, t2.y, t3.x, t3.y);
+  }
+}
+
+// hq[i] = (H_hi, H_lo) interleaved: one 16-byte load per element in the
+// column pass of the persistent scheduler
+static __global__ void __launch_bounds__(256) interleave_h_kernel(const float2* __restrict__ H,
+                                                           const float2* __restrict__ H_lo, float4* __restrict__ hq,
+                                                           long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 h = __ldg(H + i);
+    const float2 l = H_lo ? __ldg(H_lo + i) : make_float2(0.f, 0.f);
+    hq[i] = make_float4(h.x, h.y, l.x, l.y);
   }
 }
 

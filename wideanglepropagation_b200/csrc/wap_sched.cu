@@ -34,6 +34,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "wap_internal.h"
@@ -43,10 +45,11 @@ namespace wap {
 
 constexpr int kSchedThreads = 256;
 constexpr int kMaxClasses = 4;
-constexpr int kTileBytes = 32 * 1024;                 // every tile is 32 KB
-constexpr int kExchBytes = 36 * 1024;                 // >= rows * padded(n) * 8
+// A tile is 256 compute threads x E elements (complex64): 32 KB for E = 16,
+// 16 KB for E = 8; the exchange buffer holds rows x padded(n) of a row tile.
+__host__ __device__ constexpr int kTileBytesFor(int e) { return 256 * e * 8; }
+__host__ __device__ constexpr int kExchBytesFor(int e) { return 256 * e * 8 + 256 * e * 8 / 16; }
 constexpr long long kSpinLimit = 1LL << 22;           // polls before a wait gives up
-constexpr int kSchedE = 16;                           // elements per thread (all sizes)
 
 struct SchedClass {
   int n, log2n, n_slices, n_probes;
@@ -60,12 +63,12 @@ struct SchedClass {
   const int* draw;              // (B) or null
   const float2* ttab;           // (draws, N, n, n)
   long long ttab_draw_stride;   // N n n
-  const float2* H;
-  const float2* H_lo;           // or null
+  const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
   float* dp;                    // (B, n, n) or null
   const float4* tw;             // twiddles for (n, 16) in global memory
   int tw_off, tw_len;           // their place in the shared-memory copy
-  float scale;                  // 1 / (n n)
+  float scale;                  // 1 / (n n)  (also folded into ttab)
+  float inv_scale;              // n n
 };
 
 struct SchedDesc {
@@ -86,6 +89,7 @@ struct alignas(64) SchedParams {
   long long spin_limit;            // polls before a wait gives up
   int stall_pass;                  // test hook: tiles of this pass wait forever (-1: off)
   int checks;                      // validate every task before use (debug)
+  int tw_in_smem;                  // twiddles copied to shared memory (else read via L1)
   int* debug;                      // [code, cls, pass, b, tile, extra] of the first bad task
 };
 
@@ -189,9 +193,8 @@ constexpr int kBlockThreads = kSchedThreads + 32;       // + 1 producer warp
 constexpr int kFftBar = 2;                              // named barrier of the compute warps
 
 // Row tile, phase 1: this thread's E input words into registers.
-template <int N>
-__device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, const float2* stage, float2 (&v)[kSchedE]) {
-  constexpr int E = kSchedE;
+template <int N, int E>
+__device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, const float2* stage, float2 (&v)[E]) {
   constexpr int T = N / E;
   const int rl = threadIdx.x / T, t = threadIdx.x - rl * T;
   if (k.pass == 0) {
@@ -213,18 +216,26 @@ __device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, con
 }
 
 // Row tile, phase 2: [inverse row FFT, scale], [* t_s, forward row FFT], store.
-template <int N>
-__device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, float2 (&v)[kSchedE], float2* exch,
+template <int N, int E>
+__device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, float2 (&v)[E], float2* exch,
                                             const float4* tw) {
-  constexpr int E = kSchedE;
   constexpr int T = N / E;
   constexpr int PADN = RowExchange<true>::padded(N);
   const int rl = threadIdx.x / T, t = threadIdx.x - rl * T;
   const int row = k.tile * c.rows + rl;
   const long long plane = (long long)N * N;
   const RowExchange<(T <= 32), kFftBar, kSchedThreads> xs{exch + rl * PADN};
+  // ttab holds t / (n n): the inverse transform's normalisation rides on the
+  // transmission multiply; the first pass (no inverse transform) undoes it
+  // and the last pass (no transmission) applies it.  All factors are powers
+  // of two, so this changes no rounding.
   if (k.pass != 0) {
     fft<N, E, true>(v, t, xs, tw);
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
+  }
+  if (k.pass == 2 * c.n_slices) {
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.scale);
   }
@@ -241,9 +252,8 @@ __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, 
   for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
 }
 
-template <int N>
-__device__ __forceinline__ void col_load(const SchedClass& c, const float2* stage, float2 (&v)[kSchedE]) {
-  constexpr int E = kSchedE;
+template <int N, int E>
+__device__ __forceinline__ void col_load(const SchedClass& c, const float2* stage, float2 (&v)[E]) {
   constexpr int T = N / E;
   constexpr int W = kSchedThreads / T;
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
@@ -252,10 +262,9 @@ __device__ __forceinline__ void col_load(const SchedClass& c, const float2* stag
 }
 
 // Column tile: FFT, * H (hi + lo), [dp on the last slice], inverse FFT, store.
-template <int N>
-__device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, float2 (&v)[kSchedE], float2* exch,
+template <int N, int E>
+__device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, float2 (&v)[E], float2* exch,
                                             const float4* tw) {
-  constexpr int E = kSchedE;
   constexpr int T = N / E;
   constexpr int W = kSchedThreads / T;
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
@@ -263,17 +272,11 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
   const long long plane = (long long)N * N;
   const ColExchange<kFftBar, kSchedThreads> xs{exch, W, cc};
   fft<N, E, false>(v, t, xs, tw);
-  const float2* hcol = c.H + col;
-  if (c.H_lo) {
-    const float2* lcol = c.H_lo + col;
+  const float4* hcol = c.Hq + col;
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int o = (t + T * e) * N;
-      v[e] = cmul_hl(v[e], __ldg(hcol + o), __ldg(lcol + o));
-    }
-  } else {
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(hcol + (t + T * e) * N));
+  for (int e = 0; e < E; ++e) {
+    const float4 h = __ldg(hcol + (t + T * e) * N);
+    v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
   }
   if (c.dp && (k.pass >> 1) == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
@@ -303,32 +306,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long lo
   return true;
 }
 
-// OR of a predicate over the compute warps (named barrier kFftBar)
-__device__ __forceinline__ bool compute_any(bool p) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred q, r;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred r, %2, %3, q;\n selp.u32 %0, 1, 0, r;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)p), "n"(kFftBar), "n"(kSchedThreads)
-      : "memory");
-  return r != 0;
-}
-
 // Compute warps: take the published tile, pull it into registers, release the
 // stage, run the transforms, store, report completion.
-template <unsigned MASK>
+template <unsigned MASK, int E>
 __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage, float2* exch, const float4* tw_smem,
                                              uint64_t* full, uint64_t* empty, uint64_t* done_bar, const Task* s_task) {
   uint32_t fph = 0;
   uint32_t tiles_done = 0;   // selects the done barrier (two, alternating)
   const int lane = threadIdx.x & 31;
   while (true) {
-    const bool late = !mbar_wait(full, fph, P.spin_limit);
+    // Bounded wait for the next published item.  On expiry record the error
+    // and keep waiting (bounded rounds): the producer's own waits are bounded
+    // and it publishes the stop sentinel once an error is recorded, so every
+    // compute warp reads the same item and runs the same barrier sequence.
+    for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit); ++round)
+      atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
     fph ^= 1u;
-    if (compute_any(late)) {
-      if (threadIdx.x == 0) atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
-      return;
-    }
     const Task k = *s_task;
     if (!k.valid) return;
     if (!task_ok(P, k, 1)) {
@@ -341,17 +334,17 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
       continue;
     }
     const SchedClass& c = P.cls[k.cls];
-    const float4* tw = tw_smem + c.tw_off;
-    float2 v[kSchedE];
+    const float4* tw = P.tw_in_smem ? tw_smem + c.tw_off : c.tw;
+    float2 v[E];
 #define WAP_SCHED_CASE(N, BIT)                                  \
     if constexpr ((MASK & BIT) != 0) {                            \
       if (c.n == N) {                                             \
-        if (k.pass & 1) col_load<N>(c, stage, v);                 \
-        else row_load<N>(c, k, stage, v);                         \
+        if (k.pass & 1) col_load<N, E>(c, stage, v);              \
+        else row_load<N, E>(c, k, stage, v);                      \
         __syncwarp();                                             \
         if (lane == 0) mbar_arrive(empty);                        \
-        if (k.pass & 1) col_compute<N>(c, k, v, exch, tw);        \
-        else row_compute<N>(c, k, v, exch, tw);                   \
+        if (k.pass & 1) col_compute<N, E>(c, k, v, exch, tw);     \
+        else row_compute<N, E>(c, k, v, exch, tw);                \
       }                                                           \
     }
     WAP_SCHED_CASE(128, 1u)
@@ -368,18 +361,21 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
 // ---------------------------------------------------------------------------
 // the persistent kernel: 8 compute warps + 1 producer warp
 // ---------------------------------------------------------------------------
-template <unsigned MASK>
-__global__ void __launch_bounds__(kBlockThreads, 2) scan_kernel(const __grid_constant__ SchedParams P) {
+template <unsigned MASK, int E>
+__global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(const __grid_constant__ SchedParams P) {
   extern __shared__ __align__(1024) unsigned char sched_smem[];
   float2* stage = reinterpret_cast<float2*>(sched_smem);
-  float2* exch = reinterpret_cast<float2*>(sched_smem + kTileBytes);
-  float4* tw_smem = reinterpret_cast<float4*>(sched_smem + kTileBytes + kExchBytes);
+  constexpr int kTile = kTileBytesFor(E), kExch = kExchBytesFor(E);
+  float2* exch = reinterpret_cast<float2*>(sched_smem + kTile);
+  float4* tw_smem = reinterpret_cast<float4*>(sched_smem + kTile + kExch);
   __shared__ __align__(8) uint64_t full, empty, done_bar[2];
   __shared__ Task s_task;
 
-  for (int ci = 0; ci < P.n_classes; ++ci) {
-    const SchedClass& c = P.cls[ci];
-    for (int i = threadIdx.x; i < c.tw_len; i += blockDim.x) tw_smem[c.tw_off + i] = c.tw[i];
+  if (P.tw_in_smem) {
+    for (int ci = 0; ci < P.n_classes; ++ci) {
+      const SchedClass& c = P.cls[ci];
+      for (int i = threadIdx.x; i < c.tw_len; i += blockDim.x) tw_smem[c.tw_off + i] = c.tw[i];
+    }
   }
   if (threadIdx.x == 0) {
     mbar_init(&full, 1);
@@ -391,7 +387,7 @@ __global__ void __launch_bounds__(kBlockThreads, 2) scan_kernel(const __grid_con
   __syncthreads();
 
   if (threadIdx.x < kSchedThreads) {
-    compute_loop<MASK>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
+    compute_loop<MASK, E>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
     return;
   }
 
@@ -517,21 +513,27 @@ using namespace wap;
 
 typedef void (*ScanKernel)(const SchedParams);
 
-// kernel instances by the set of grid sizes they contain (bit 0: 128,
-// 1: 256, 2: 512, 3: 1024); other sets use the all-sizes instance
-static ScanKernel pick_scan_kernel(unsigned mask) {
+// kernel instances by elements per thread and the set of grid sizes they
+// contain (bit 0: 128, 1: 256, 2: 512, 3: 1024); other sets use the
+// all-sizes instance
+template <int E>
+static ScanKernel pick_scan_kernel_e(unsigned mask) {
   switch (mask) {
-    case 1u: return scan_kernel<1u>;
-    case 2u: return scan_kernel<2u>;
-    case 4u: return scan_kernel<4u>;
-    case 8u: return scan_kernel<8u>;
-    case 6u: return scan_kernel<6u>;
-    default: return scan_kernel<15u>;
+    case 1u: return scan_kernel<1u, E>;
+    case 2u: return scan_kernel<2u, E>;
+    case 4u: return scan_kernel<4u, E>;
+    case 8u: return scan_kernel<8u, E>;
+    case 6u: return scan_kernel<6u, E>;
+    default: return scan_kernel<15u, E>;
   }
+}
+static ScanKernel pick_scan_kernel(unsigned mask, int e) {
+  return e == 8 ? pick_scan_kernel_e<8>(mask) : pick_scan_kernel_e<16>(mask);
 }
 
 struct wap_scan {
   ScanKernel kernel = nullptr;
+  int e = 16;
   int device = 0;
   int n_classes = 0;
   SchedParams params{};
@@ -545,6 +547,7 @@ struct wap_scan {
   size_t smem = 0;
   std::vector<float4*> d_tw;
   std::vector<float2*> d_ttab;
+  std::vector<float4*> d_hq;
   std::vector<size_t> ttab_elems;
   std::vector<wap_scan_class> cls;
   std::vector<Physics> phys;
@@ -572,6 +575,7 @@ static void scan_free(wap_scan* s) {
   cudaFree(s->d_debug);
   for (auto p : s->d_tw) cudaFree(p);
   for (auto p : s->d_ttab) cudaFree(p);
+  for (auto p : s->d_hq) cudaFree(p);
   delete s;
 }
 
@@ -594,6 +598,12 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
   cudaError_t e;
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  // elements per thread of the scheduler's transforms
+  int E = 16;
+  if (const char* ov = getenv("WAP_SCHED_E")) {   // debugging / A-B timing only
+    if (!strcmp(ov, "8")) E = 8;
+  }
+  s->e = E;
   unsigned mask = 0;
   int tw_total = 0;
   for (int ci = 0; ci < n_classes; ++ci) {
@@ -603,10 +613,20 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
       return fail(WAP_ERR_UNSUPPORTED, "scan grids must be 128, 256, 512 or 1024 (got %d)", n);
     }
     mask |= n == 128 ? 1u : n == 256 ? 2u : n == 512 ? 4u : 8u;
-    tw_total += make_plan_shape(n, kSchedE).tw_size();
+    tw_total += make_plan_shape(n, E).tw_size();
   }
-  s->kernel = pick_scan_kernel(mask);
-  s->smem = kTileBytes + kExchBytes + (size_t)tw_total * sizeof(float4);
+  s->kernel = pick_scan_kernel(mask, E);
+  // Keep the twiddles in shared memory only when they fit next to the stage
+  // and exchange buffers without lowering the CTAs per SM (3 for E = 16,
+  // 4 for E = 8).
+  const size_t base_smem = kTileBytesFor(E) + kExchBytesFor(E);
+  const int want_ctas = E == 16 ? 3 : 4;
+  s->params.tw_in_smem = want_ctas * (base_smem + (size_t)tw_total * sizeof(float4) + 1024) <= 227 * 1024;
+  if (const char* ov = getenv("WAP_SCHED_TWIDDLES")) {   // debugging / A-B timing only
+    if (!strcmp(ov, "smem")) s->params.tw_in_smem = 1;
+    if (!strcmp(ov, "global")) s->params.tw_in_smem = 0;
+  }
+  s->smem = base_smem + (s->params.tw_in_smem ? (size_t)tw_total * sizeof(float4) : 0);
   if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem)) != cudaSuccess) {
     scan_free(s);
     return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
@@ -628,7 +648,7 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
       scan_free(s);
       return fail(WAP_ERR_ARG, "scan class %d: bad sizes or NULL V/psi0/H/exit", ci);
     }
-    const int n = c.n, T = n / kSchedE;
+    const int n = c.n, T = n / E;
     SchedClass& sc = s->params.cls[ci];
     sc.n = n;
     sc.log2n = ilog2c(n);
@@ -644,13 +664,19 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
     sc.psi0 = reinterpret_cast<const float2*>(c.psi0);
     sc.positions = c.positions;
     sc.draw = c.draw;
-    sc.H = reinterpret_cast<const float2*>(c.H);
-    sc.H_lo = reinterpret_cast<const float2*>(c.H_lo);
+    float4* dhq = nullptr;
+    if ((e = cudaMalloc(&dhq, (size_t)n * n * sizeof(float4))) != cudaSuccess) {
+      scan_free(s);
+      return cuda_fail(e, "cudaMalloc(interleaved H)");
+    }
+    s->d_hq.push_back(dhq);
+    sc.Hq = dhq;
     sc.dp = c.dp;
     sc.scale = (float)(1.0 / ((double)n * n));
+    sc.inv_scale = (float)((double)n * n);
     sc.ttab_draw_stride = (long long)c.n_slices * n * n;
     // twiddles
-    std::vector<float4> h = twiddle_table(n, kSchedE);
+    std::vector<float4> h = twiddle_table(n, E);
     float4* dtw = nullptr;
     if ((e = cudaMalloc(&dtw, h.size() * sizeof(float4))) != cudaSuccess ||
         (e = cudaMemcpy(dtw, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice)) != cudaSuccess) {
@@ -759,9 +785,16 @@ int wap_scan_run(wap_scan* s, void* stream) {
     const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
     count_launch();
     trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
-        s->cls[ci].V, s->d_ttab[ci], n4, (float)ph.ri_a, (float)ph.ri_inv_den, (float)ph.kphase);
+        s->cls[ci].V, s->d_ttab[ci], n4, (float)ph.ri_a, (float)ph.ri_inv_den, (float)ph.kphase,
+        s->params.cls[ci].scale);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
     prof_end(tok, st, 12.0 * (double)s->ttab_elems[ci]);
+    const long long nn = (long long)s->cls[ci].n * s->cls[ci].n;
+    count_launch();
+    interleave_h_kernel<<<(unsigned)std::min<long long>((nn + 255) / 256, 148LL * 8), 256, 0, st>>>(
+        reinterpret_cast<const float2*>(s->cls[ci].H), reinterpret_cast<const float2*>(s->cls[ci].H_lo),
+        s->d_hq[ci], nn);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "interleave_h_kernel");
   }
   // algorithmic bytes of a slice step: wave in 8 + wave out 8 + potential 4
   // per pixel (the two passes' intermediate round trip is not counted)

@@ -190,7 +190,7 @@ class BatchedScan:
 
     def launches(self) -> int:
         if self.mode == "persistent":
-            return len(self.classes) + 1
+            return 2 * len(self.classes) + 1
         if self.mode == "plain" and self.plain_subset is not None:
             return sum((2 * c.n_slices + 1) * min(self.plain_subset, c.n_probes) for c in self.classes)
         return launches_per_step(self.classes, "plain" if self.mode == "plain" else "batched")
