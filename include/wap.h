@@ -125,6 +125,23 @@ int wap_multislice_bwd(wap_plan* plan, const float* V, int n_slices, int n_draws
                        const float* grad_dp, const float* grad_exit, float* grad_V,
                        float* work, void* stream);
 
+/* Fresnel / angular-spectrum forward that allocates no device memory.  No
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * when they run (recording a CUDA graph under a framework that forbids
+ * allocation during capture, fixed-pool hosts, plugin hosts that only pass
+ * in/out buffers).  Same arguments and results as wap_multislice_fwd without
+ * the plan (ny x nx given explicitly, one potential draw, default launch
+ * shape, transmission evaluated per probe).  The FFT twiddle tables live in a
+ * fixed 128 KiB array inside the library (held by every GPU that loads it
+ * until exit) and are rewritten by each call; calls that overlap on the GPU
+ * share that array and race.  The first call on a device looks up the array's
+ * device address: make it before any stream capture.  Grids whose tables do
+ * not fit are rejected with WAP_ERR_UNSUPPORTED. */
+int wap_multislice_fwd_noalloc(const float* V, int n_slices, int ny, int nx, const float* psi0,
+                               int n_probes, int psi0_per_probe, const int32_t* positions,
+                               const float* H, const float* H_lo, double dz, double energy,
+                               float* exit, float* dp, float* stack, void* stream);
+
 /* Batched scan: one grid class of probes (square n x n grid, n in
  * {128, 256, 512, 1024}) with its own potential draws, probe and propagator.
  * All pointers are device pointers; the probe is shared and rolled to each

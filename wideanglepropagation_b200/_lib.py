@@ -41,6 +41,7 @@ SIGNATURES = {
     "wap_wpm_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _D, _D, _D, _D, _D, _P, _P, _P, _P]),
     "wap_multislice_fwd_ckpt": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _I, _P]),
     "wap_multislice_bwd": (_I, [_P, _P, _I, _I, _P, _I, _P, _P, _D, _D, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "wap_multislice_fwd_noalloc": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "wap_scan_create": (_I, [ctypes.POINTER(_P), _I, _P]),
     "wap_scan_run": (_I, [_P, _P]),
     "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
