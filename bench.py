@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--impl", default="wap", choices=["wap", "reference"])
     ap.add_argument("--small", action="store_true", help="tiny workload (testing the harness)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/grad/err/cpu sections")
+    ap.add_argument("--profile-grad", action="store_true",
+                    help="gradient case for ncu captures: 64 probes 256^2 x 16 slices, checkpoint every 4, one "
+                         "forward + backward through the persistent scheduler")
     ap.add_argument("--mode", default="persistent", choices=["persistent", "batched", "graph"],
                     help="batched execution mode timed as the headline")
     ap.add_argument("--profile-case", action="store_true",
@@ -158,8 +161,31 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- GPU side
+def profile_grad():
+    import torch
+    import wideanglepropagation_b200 as wap
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    w = wap.synthetic.inverse_problem(0, n=256, n_slices=16, n_side=8)
+    dev = torch.device("cuda", 0)
+    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    probe = torch.as_tensor(w.probe).to(dev)
+    pos = torch.as_tensor(w.positions).to(dev)
+    Vt = torch.as_tensor(w.potential[0]).to(dev)
+    _, target, _ = wap.simulate_fresnel_as(Vt, probe, H, w.dz, w.energy, positions=pos, return_wavefronts=False)
+    V = torch.zeros_like(Vt, requires_grad=True)
+    for _ in range(2):
+        V.grad = None
+        _, dp = simulate_fresnel_as_differentiable(V, probe, H, w.dz, w.energy, positions=pos, ckpt_every=4)
+        ((dp - target) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_grad": "ok", "grad_norm": float(V.grad.norm())}))
+
+
 def main():
     args = parse()
+    if args.profile_grad:
+        profile_grad()
+        return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
     if args.profile_case:
@@ -260,6 +286,7 @@ def main():
     if not args.no_extras and rank == 0:
         extras.update(_plain(classes, args))
         extras.update(_per_pass(classes, args))
+        extras.update(_configs())
         extras.update(_grad_ratio(args))
         extras.update(_err_vs_fp64(classes, classes_host))
 
@@ -336,6 +363,50 @@ def _plain(classes, args):
     return {"plain": {"value": rate, "unit": "slice-steps/s", "sample": "16 probes per class, one probe per launch"},
             "per_class_slice_steps_per_s": {f"{c.ny}x{c.nx}": {"batched": 1 / b, "plain": 1 / p}
                                             for c, b, p in zip(classes, bper, per)}}
+
+
+def _configs():
+    """Single-call timings of the other workloads through the public API
+    (inputs resident on the device), with their error vs the FP64 oracle
+    measured separately by the GPU tests."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    S = wap.synthetic
+    dev = torch.device("cuda", torch.cuda.current_device())
+    out = {}
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timeit(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    w = S.plain_fresnel(0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    ms = timeit(lambda: wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy), 20)
+    ms_ns = timeit(lambda: wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False), 20)
+    out["fresnel_256_N20_1probe"] = {"ms_per_call": ms, "ms_per_call_no_stack": ms_ns,
+                                     "slice_steps_per_s": w.n_slices / (ms_ns / 1e3)}
+    w = S.angular_spectrum_diamond(0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    ms_ns = timeit(lambda: wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False), 5)
+    out["as_1024_N100_1probe"] = {"ms_per_call_no_stack": ms_ns, "slice_steps_per_s": w.n_slices / (ms_ns / 1e3),
+                                  "pixel_slice_steps_per_s": w.n_slices * w.ny * w.nx / (ms_ns / 1e3)}
+    w = S.wpm_fcc(0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    ms_ns = timeit(lambda: wap.simulate_wpm(V, pr, w.dz, w.energy, (w.ps, w.ps), 16, 1.0, return_wavefronts=False), 2)
+    out["wpm_512_N200_K16_1probe"] = {"ms_per_call_no_stack": ms_ns, "slice_steps_per_s": w.n_slices / (ms_ns / 1e3)}
+    return {"configs": out}
 
 
 def _per_pass(classes, args):

@@ -115,3 +115,55 @@ def test_grad_with_draws(wap):
         sel = np.nonzero(draw == d)[0]
         _, gr = T.loss_and_grad(V2[d], probe, H, dz, E, target[sel], pos[sel])
         assert np.linalg.norm(g[d] - gr) / np.linalg.norm(gr) < 1e-4
+
+
+def _scan_problem(n=128, N=9, n_side=3, seed=4):
+    import wideanglepropagation_b200.synthetic as S
+    from oracle import propagation_oracle as O
+    from oracle import torch_oracle as T
+    rng = np.random.default_rng(seed)
+    ps, dz, E = 0.08, 2.0, 300e3
+    Vt = S.random_gaussian_stack(rng, N, n, n, ps, 6, 20.0, 0.3) / dz
+    V0 = 0.5 * (S.random_gaussian_stack(rng, N, n, n, ps, 6, 20.0, 0.3) / dz)
+    probe = S.aperture_probe(n, n, ps, E, 25.0, -50.0, dtype=np.complex64)
+    pos = S.raster_positions(n, n, n_side, n_side)
+    H = O.angular_spectrum_propagation_kernel(n, n, (ps, ps), dz, E)
+    _, target = T.simulate(torch.tensor(Vt), probe, H, dz, E, pos)
+    return V0, probe, pos, H, dz, E, target.numpy()
+
+
+@pytest.mark.parametrize("ckpt", [1, 3, 4, 9])
+def test_persistent_gradient_matches_autograd(wap, ckpt):
+    """>= 8 probes on a 128^2 grid: forward, checkpoints, recompute and adjoint
+    all run in the persistent scheduler."""
+    from oracle import torch_oracle as T
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    V0, probe, pos, H, dz, E, target = _scan_problem()
+    assert len(pos) >= 8
+    L_ref, g_ref = T.loss_and_grad(V0, probe, H, dz, E, target, pos)
+    V = torch.tensor(V0, dtype=torch.float32, device="cuda", requires_grad=True)
+    _, dp = simulate_fresnel_as_differentiable(V, probe, H, dz, E, positions=pos, ckpt_every=ckpt)
+    L = ((dp - torch.tensor(target, device="cuda", dtype=torch.float32)) ** 2).sum()
+    L.backward()
+    err = np.linalg.norm(V.grad.cpu().numpy() - g_ref) / np.linalg.norm(g_ref)
+    assert abs(float(L) - L_ref) / L_ref < 1e-4
+    assert err < 1e-4, err
+
+
+def test_persistent_gradient_two_pending_graphs(wap):
+    """Two forwards before their backwards get separate scan buffers."""
+    from oracle import torch_oracle as T
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    V0, probe, pos, H, dz, E, target = _scan_problem(N=5, seed=6)
+    tgt = torch.tensor(target, device="cuda", dtype=torch.float32)
+    V = torch.tensor(V0, dtype=torch.float32, device="cuda", requires_grad=True)
+    _, dp1 = simulate_fresnel_as_differentiable(V, probe, H, dz, E, positions=pos, ckpt_every=2)
+    _, dp2 = simulate_fresnel_as_differentiable(V * 0.5, probe, H, dz, E, positions=pos, ckpt_every=2)
+    (((dp1 - tgt) ** 2).sum() + ((dp2 - tgt) ** 2).sum()).backward()
+    Vr = torch.tensor(V0, requires_grad=True)
+    _, d1 = T.simulate(Vr, probe, H, dz, E, pos)
+    _, d2 = T.simulate(Vr * 0.5, probe, H, dz, E, pos)
+    tr = torch.tensor(target)
+    (((d1 - tr) ** 2).sum() + ((d2 - tr) ** 2).sum()).backward()
+    err = np.linalg.norm(V.grad.cpu().numpy() - Vr.grad.numpy()) / np.linalg.norm(Vr.grad.numpy())
+    assert err < 1e-4, err

@@ -44,6 +44,9 @@ SIGNATURES = {
     "wap_multislice_fwd_noalloc": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
     "wap_scan_create": (_I, [ctypes.POINTER(_P), _I, _P]),
     "wap_scan_run": (_I, [_P, _P]),
+    "wap_scan_grad_create": (_I, [ctypes.POINTER(_P), _P, _I]),
+    "wap_scan_grad_backward": (_I, [_P, _P, _P, _P]),
+    "wap_scan_bind": (_I, [_P, _I, _P]),
     "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
     "wap_scan_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_scan_destroy": (_I, [_P]),

@@ -452,6 +452,31 @@ cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t 
   return cudaSuccess;
 }
 
+// exp(i phi(V)) for every draw and slice into the plan's grow-only table
+int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st) {
+  const size_t need = (size_t)n_draws * n_slices * p->ny * p->nx;
+  cudaError_t e = cudaSuccess;
+  if (need > p->ttab_cap) {
+    cudaFree(p->ttab);
+    p->ttab = nullptr;
+    p->ttab_cap = 0;
+    e = cudaMalloc(&p->ttab, need * sizeof(float2));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return cuda_fail(e, "cudaMalloc(transmission table)");
+    }
+    p->ttab_cap = need;
+  }
+  const long long n4 = (long long)need / 4;
+  const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
+  count_launch();
+  trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
+      V, p->ttab, n4, r.ri_a, r.ri_inv_den, r.kphase);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
+  prof_end(tok, st, 12.0 * (double)need);
+  return WAP_OK;
+}
+
 // Forward multislice; snapshots of the wave entering slice s go to
 // snap + (s / snap_every) * plane when s % snap_every == 0 (snap_first = 0:
 // checkpoints), or the wave after every slice to stack (snap_first = 1).
@@ -477,29 +502,11 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   // When several probes see each potential slice, tabulate exp(i phi(V)) once
   // per (draw, slice) instead of evaluating it per probe.
   int trans_flag = ROW_TRANS;
-  if (n_probes >= 2 * n_draws) {
-    const size_t need = (size_t)n_draws * n_slices * plane;
-    cudaError_t e = cudaSuccess;
-    if (need > p->ttab_cap) {
-      cudaFree(p->ttab);
-      p->ttab = nullptr;
-      p->ttab_cap = 0;
-      e = cudaMalloc(&p->ttab, need * sizeof(float2));
-      if (e == cudaSuccess) p->ttab_cap = need;
-    }
-    if (e == cudaSuccess) {
-      const long long n4 = (long long)need / 4;
-      const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
-      count_launch();
-      trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
-          V, p->ttab, n4, r.ri_a, r.ri_inv_den, r.kphase);
-      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
-      prof_end(tok, st, 12.0 * (double)need);
-      r.ttab = p->ttab;
-      trans_flag = ROW_TRANS_TAB;
-    } else {
-      cudaGetLastError();  // workspace unavailable: evaluate t per probe
-    }
+  if (n_probes >= 2 * n_draws && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) {
+    r.ttab = p->ttab;
+    trans_flag = ROW_TRANS_TAB;
+  } else {
+    clear_error();
   }
   ColArgs c = base_col_args(p, H, H_lo);
   c.psi = r.psi;
@@ -580,6 +587,11 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
   // seed: lambda_psi_N = grad_exit / 2 + F^H (g Z), Z = fft2(exit);
   // lambda_a_{N-1} = ifft2(conj(H) fft2(lambda_psi_N))
   RowArgs r = base_row_args(p, ph, V, n_slices, draw);
+  // transmission shared by the probes of a draw, for the recompute and the
+  // adjoint passes
+  const float2* ttab = nullptr;
+  if (n_probes >= 2 * n_draws && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) ttab = p->ttab;
+  else clear_error();
   r.psi = lam;
   r.psi_bstride = wstride;
   r.src = reinterpret_cast<const float2*>(exit);
@@ -611,12 +623,14 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
       q.psi = buf;
       q.psi_bstride = wstride;
       q.slice = s;
+      q.ttab = ttab;
+      const int tf = ttab ? ROW_TRANS_TAB : ROW_TRANS;
       if (s == s0) {
         q.src = ck + (long long)j * plane;
         q.src_bstride = (long long)nck * plane;
-        q.flags = ROW_LOAD_SRC | ROW_TRANS | ROW_FFT;
+        q.flags = ROW_LOAD_SRC | tf | ROW_FFT;
       } else {
-        q.flags = ROW_IFFT | ROW_TRANS | ROW_FFT;
+        q.flags = ROW_IFFT | tf | ROW_FFT;
         q.snap = seg + (long long)(s - s0) * plane;
         q.snap_bstride = wstride;
       }
@@ -651,6 +665,7 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
         a.aux_bstride = wstride;
       }
       a.grad = grad_V;
+      a.ttab = ttab;
       if ((e = row_chunks(p, a, n_probes, st)) != cudaSuccess) return cuda_fail(e, "adjoint row pass");
       if (s == 0) break;
       ColArgs ca = base_col_args(p, H, H_lo);

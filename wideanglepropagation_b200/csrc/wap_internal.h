@@ -56,6 +56,7 @@ cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cud
 cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st);
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
 RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
+int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st);
 
 // kernel-level tracing (wap_prof.cu)
 struct ProfToken {

@@ -232,14 +232,21 @@ row_pass_kernel(const RowArgs a) {
       //   lambda_psi_s = conj(t_s) lambda_a
       const float2* arow = a.aux + (long long)b * a.aux_bstride + (long long)row * NX;
       float* grow = a.grad + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
+      const float2* trow =
+          a.ttab ? a.ttab + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX : nullptr;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int x = t + T * e;
         const float vv = __ldg(vrow + x);
         const float dn = refr_minus_one(vv, a.ri_a, a.ri_inv_den);
-        float s, c;
-        sincosf(a.kphase * dn, &s, &c);
-        const float2 tt = make_float2(c, s);
+        float2 tt;
+        if (trow) {
+          tt = __ldg(trow + x);   // shared transmission table (unscaled)
+        } else {
+          float s, c;
+          sincosf(a.kphase * dn, &s, &c);
+          tt = make_float2(c, s);
+        }
         const float2 as = cmul(__ldcg(arow + x), tt);
         const float dphidv = a.kphase * (a.e_plus_e0 + vv) * a.ri_inv_den / (1.0f + dn);
         const float gre = 2.0f * (v[e].y * as.x - v[e].x * as.y) * dphidv;

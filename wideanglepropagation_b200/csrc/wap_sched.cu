@@ -1,34 +1,51 @@
-// Persistent batched multislice scheduler (Fresnel / angular spectrum).
+// Persistent batched multislice scheduler (Fresnel / angular spectrum), and
+// the same machinery for the adjoint (gradient w.r.t. the potential).
 //
-// One launch advances every probe of every grid class of a scan through all of
-// its slices.  The work is a ticket queue: the host lays out "pass descriptors"
-// (class, probe group, pass), each expanding into probes x tiles tickets; CTAs
-// claim tickets in increasing order with one atomicAdd and run the tile:
+// One launch advances every probe of every grid class of a scan through a
+// per-probe chain of steps.  Each step is one pass over one probe's wave,
+// split into tiles: row tiles (ROWS consecutive rows) or column tiles (n rows
+// x W columns).  Forward chain (propagation.py:305-352), N slices:
 //
-//   pass 2s     (row tile: ROWS consecutive rows of one probe)
-//               s = 0: load psi0 rolled to the probe position (move_probe),
-//               else inverse row FFT of slice s-1's column output, * 1/(n n);
-//               then * t_s from the transmission table, forward row FFT
-//   pass 2s+1   (column tile: n rows x W columns of one probe)
-//               column FFT, * H (hi + lo), [dp on the last slice], inverse FFT
-//   pass 2N     (row tile) inverse row FFT -> exit wave
+//   FWD_ROW0   s = 0   psi0 rolled to the probe position (move_probe,
+//                      propagation.py:263-276) -> * t_0 -> row FFT
+//   FWD_ROW    s       inverse row FFT of slice s-1 -> * t_s -> row FFT
+//   FWD_COL    s       column FFT -> * H (hi + lo) -> [dp = |.|^2 on the last
+//                      slice] -> inverse column FFT
+//   FWD_ROWN           inverse row FFT -> exit wave
 //
-// Dependencies are per probe: a tile of pass p needs every tile of passes
-// 0..p-1 of the same probe, i.e. a per-probe completion counter >= the tile
-// count of those passes.  Tickets are ordered (class, group, pass, probe,
-// tile), so a tile only ever waits for smaller tickets, which were claimed by
-// CTAs that are running or finished: the queue cannot deadlock.  Waits are
-// bounded; on expiry the CTA records WAP_ERR_TIMEOUT, every CTA stops claiming,
+// (t_s from a table shared by the probes of a potential draw.)  The gradient
+// uses a forward that also stores the wave entering every k-th slice and the
+// whole last k-slice segment, then a backward chain
+//
+//   SEED_ROW, SEED_COL          lambda = ifft2(conj(H) n^2 g fft2(exit))
+//   per segment j (last first):
+//     REC_ROW0, REC_COL, REC_ROW, ..., REC_ROWL   recompute psi_s of the
+//                                                 segment from its checkpoint
+//                                                 (skipped for the last one)
+//     ADJ_ROW(s), ADJ_COL(s) for s = s1-1 .. s0   adjoint sweep: lambda_a =
+//       ifft2 of the column output; dL/dV_s += 2 Re(conj(lambda_a) i t psi_s)
+//       dphi/dV; lambda <- conj(t) lambda_a, row FFT; column FFT, * conj(H),
+//       inverse column FFT.
+//
+// The work is a ticket queue: the host lays out descriptors (class, probe
+// group, step), each expanding into probes x tiles tickets; a producer warp
+// per CTA claims tickets in increasing order with one atomicAdd.  A tile of
+// step p needs every tile of steps 0..p-1 of the same probe, i.e. a per-probe
+// completion counter >= the prefix tile count of step p.  Tickets are ordered
+// (class, group, step, probe, tile), so a tile only ever waits for smaller
+// tickets, claimed by CTAs that are running or finished; a CTA never blocks
+// while it holds an unsignalled tile, so the queue cannot deadlock.  Waits are
+// bounded; on expiry the CTA records WAP_ERR_TIMEOUT, CTAs stop claiming,
 // in-flight copies are drained (bounded) and the kernel returns.
 //
 // Probe groups are sized so that a group's waves stay L2-resident while the
-// group walks through its slices; groups follow each other without a barrier.
+// group walks through its chain; groups follow each other without a barrier.
 //
-// Tile loads use the Tensor Memory Accelerator: row tiles are contiguous
-// (one cp.async.bulk), column tiles are 2D boxes of a tensor map over all
-// probes' rows (cp.async.bulk.tensor.2d, no multicast).  A CTA copies the
-// landed tile into registers, immediately issues the load of its next ticket
-// into the same staging buffer, and computes the current tile meanwhile.
+// Tile loads use the Tensor Memory Accelerator: row tiles are contiguous (one
+// cp.async.bulk), column tiles are 2D boxes of a tensor map over all probes'
+// rows of a buffer (cp.async.bulk.tensor.2d, no multicast).  The producer warp
+// issues the load of the next ticket as soon as the compute warps have pulled
+// the current tile into registers, so loads overlap the transforms.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -51,21 +68,64 @@ __host__ __device__ constexpr int kTileBytesFor(int e) { return 256 * e * 8; }
 __host__ __device__ constexpr int kExchBytesFor(int e) { return 256 * e * 8 + 256 * e * 8 / 16; }
 constexpr long long kSpinLimit = 1LL << 22;           // polls before a wait gives up
 
+enum StepType : int {
+  ST_FWD_ROW0 = 0,
+  ST_FWD_ROW,
+  ST_FWD_ROWN,
+  ST_FWD_COL,
+  ST_SEED_ROW,
+  ST_SEED_COL,
+  ST_REC_ROW0,
+  ST_REC_ROW,
+  ST_REC_ROWL,
+  ST_REC_COL,
+  ST_ADJ_ROW,
+  ST_ADJ_ROW0,
+  ST_ADJ_COL,
+};
+
+__host__ __device__ constexpr bool step_is_col(int t) {
+  return t == ST_FWD_COL || t == ST_SEED_COL || t == ST_REC_COL || t == ST_ADJ_COL;
+}
+
+// buffers a column tile reads: tensor-map index
+enum BufferId : int { BUF_PSI = 0, BUF_LAM = 1, BUF_WORK = 2, BUF_COUNT = 3 };
+
+struct Step {
+  int type;
+  int slice;
+  int seg0;       // first slice of the step's checkpoint segment
+  int ckpt_slot;  // forward rows: checkpoint slot written (-1: none); REC_ROW0: slot read
+  int seg_slot;   // forward/recompute rows: segment slot written; ADJ rows: slot read
+  int prefix;     // tiles of all earlier steps of the probe
+};
+
 struct SchedClass {
   int n, log2n, n_slices, n_probes;
   int rows, cols_w;             // row-tile height, column-tile width
-  int row_tiles, col_tiles;     // tiles per probe per pass
+  int row_tiles, col_tiles;     // tiles per probe per step
   int box_rows;                 // TMA box height for column tiles (<= 256)
   int done_off;                 // offset of this class's counters
+  const Step* steps;            // the per-probe chain
   float2* psi;                  // (B, n, n) working buffer / exit
   const float2* psi0;           // (n, n) shared probe
   const int* positions;         // (B, 2) or null
   const int* draw;              // (B) or null
-  const float2* ttab;           // (draws, N, n, n)
-  long long ttab_draw_stride;   // N n n
+  const float* V;               // (draws, N, n, n) volts (adjoint only)
+  const float2* ttab;           // (draws, N, n, n)  t / (n n)
+  long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
   float* dp;                    // (B, n, n) or null
-  const float4* tw;             // twiddles for (n, 16) in global memory
+  // gradient buffers
+  float2* lam;                  // (B, n, n) adjoint state
+  float2* work;                 // (B, n, n) recompute buffer
+  float2* seg;                  // (B, k, n, n) waves of the current segment
+  float2* ckpt;                 // (B, nck, n, n) checkpoints
+  int ckpt_n, seg_n;            // slots per probe
+  const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp
+  float* grad;                  // (draws, N, n, n) dL/dV, accumulated
+  float ri_a, ri_inv_den, kphase, e_plus_e0;
+  const float4* tw;             // twiddles for (n, E) in global memory
   int tw_off, tw_len;           // their place in the shared-memory copy
   float scale;                  // 1 / (n n)  (also folded into ttab)
   float inv_scale;              // n n
@@ -77,7 +137,7 @@ struct SchedDesc {
 };
 
 struct alignas(64) SchedParams {
-  CUtensorMap maps[kMaxClasses];   // column-tile tensor maps (one per class)
+  CUtensorMap maps[kMaxClasses][BUF_COUNT];   // column-tile tensor maps
   SchedClass cls[kMaxClasses];
   const SchedDesc* desc;
   int n_desc;
@@ -87,10 +147,11 @@ struct alignas(64) SchedParams {
   int* done;                       // per-probe completed tiles
   int* status;                     // 0 or WAP_ERR_TIMEOUT
   long long spin_limit;            // polls before a wait gives up
-  int stall_pass;                  // test hook: tiles of this pass wait forever (-1: off)
+  int stall_pass;                  // test hook: tiles of this step wait forever (-1: off)
   int checks;                      // validate every task before use (debug)
   int tw_in_smem;                  // twiddles copied to shared memory (else read via L1)
-  int* debug;                      // [code, cls, pass, b, tile, extra] of the first bad task
+  int stage2;                      // a second staging buffer: adjoint rows get psi_s by TMA too
+  int* debug;                      // [code, cls, step, b, tile, extra] of the first bad task
 };
 
 // ---------------------------------------------------------------------------
@@ -105,6 +166,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
   uint32_t ok;
   asm volatile(
@@ -113,6 +177,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
       : "r"(smem_u32(bar)), "r"(phase)
       : "memory");
   return ok != 0;
+}
+// bounded mbarrier wait; false if the limit expired
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit) {
+  long long spins = 0;
+  while (!mbar_try_wait(bar, phase)) {
+    if (++spins > limit) return false;
+  }
+  return true;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -135,26 +207,43 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
-// tile bodies
+// tasks
 // ---------------------------------------------------------------------------
 struct Task {
   int cls, pass, b, tile, valid;
 };
 
-// tiles of passes 0..p-1 of one probe (row passes are the even ones)
-__device__ __forceinline__ int tiles_before(const SchedClass& c, int p) {
-  return ((p + 1) >> 1) * c.row_tiles + (p >> 1) * c.col_tiles;
+// Step of the plain forward chain, decoded from the pass index alone: rows on
+// even passes (first one loads the probe, last one finishes the exit wave),
+// columns on odd passes.
+__device__ __forceinline__ Step forward_step(const SchedClass& c, int pass) {
+  Step st;
+  st.slice = pass >> 1;
+  st.type = (pass & 1) ? ST_FWD_COL : pass == 0 ? ST_FWD_ROW0 : pass == 2 * c.n_slices ? ST_FWD_ROWN : ST_FWD_ROW;
+  st.seg0 = 0;
+  st.ckpt_slot = -1;
+  st.seg_slot = -1;
+  st.prefix = ((pass + 1) >> 1) * c.row_tiles + (pass >> 1) * c.col_tiles;
+  return st;
+}
+
+template <bool GRAD>
+__device__ __forceinline__ Step step_of(const SchedClass& c, int pass) {
+  if constexpr (GRAD) return c.steps[pass];
+  else return forward_step(c, pass);
 }
 
 // Debug validation of a decoded task (P.checks): record the first violation
 // and report whether the task may be used.
+template <bool GRAD>
 __device__ __forceinline__ bool task_ok(const SchedParams& P, const Task& k, int where) {
   if (!P.checks) return true;
   bool ok = k.cls >= 0 && k.cls < P.n_classes;
   if (ok) {
     const SchedClass& c = P.cls[k.cls];
-    ok = k.b >= 0 && k.b < c.n_probes && k.pass >= 0 && k.pass <= 2 * c.n_slices && k.tile >= 0 &&
-         k.tile < ((k.pass & 1) ? c.col_tiles : c.row_tiles);
+    const int type = step_of<GRAD>(c, k.pass).type;
+    ok = k.b >= 0 && k.b < c.n_probes && k.pass >= 0 && k.tile >= 0 &&
+         k.tile < (step_is_col(type) ? c.col_tiles : c.row_tiles);
   }
   if (!ok && atomicCAS(P.debug, 0, where) == 0) {
     P.debug[1] = k.cls;
@@ -166,38 +255,62 @@ __device__ __forceinline__ bool task_ok(const SchedParams& P, const Task& k, int
   return ok;
 }
 
+__device__ __forceinline__ uint32_t tile_bytes(const SchedClass& c, int type) {
+  if (type == ST_FWD_ROW0) return 0;   // loaded directly (rolled probe)
+  return step_is_col(type) ? (uint32_t)(c.n * c.cols_w * 8) : (uint32_t)(c.rows * c.n * 8);
+}
+
 // Issue the TMA load of a task's input tile into `stage` (one thread).  This
 // is the single arrival of the phase on `bar`: arrive.expect_tx(tile bytes),
-// completed by the copy.  Returns false (no arrival) for tasks that load their
-// input directly (first row pass).
-__device__ __forceinline__ bool issue_load(const SchedParams& P, const Task& k, float2* stage, uint64_t* bar) {
+// completed by the copy.  Not called for tasks that load directly.
+template <bool GRAD>
+__device__ __forceinline__ void issue_load(const SchedParams& P, const Task& k, float2* stage, uint64_t* bar) {
   const SchedClass& c = P.cls[k.cls];
+  const Step st = step_of<GRAD>(c, k.pass);
   const long long plane = (long long)c.n * c.n;
-  if ((k.pass & 1) == 0) {
-    if (k.pass == 0) return false;
-    const float2* src = c.psi + (long long)k.b * plane + (long long)k.tile * c.rows * c.n;
-    const uint32_t bytes = (uint32_t)(c.rows * c.n * sizeof(float2));
-    mbar_expect_tx(bar, bytes);
-    bulk_g2s(stage, src, bytes, bar);
-  } else {
-    const uint32_t bytes = (uint32_t)(c.n * c.cols_w * sizeof(float2));
-    mbar_expect_tx(bar, bytes);
-    for (int r0 = 0; r0 < c.n; r0 += c.box_rows)
-      tma_load_2d(stage + r0 * c.cols_w, &P.maps[k.cls], k.tile * c.cols_w, k.b * c.n + r0, bar);
+  const uint32_t bytes = tile_bytes(c, st.type);
+  if (GRAD && P.stage2 && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0)) {
+    // lambda rows into the stage, the same rows of psi_s into the second stage
+    mbar_expect_tx(bar, 2 * bytes);
+    const long long roff = (long long)k.tile * c.rows * c.n;
+    bulk_g2s(stage, c.lam + (long long)k.b * plane + roff, bytes, bar);
+    bulk_g2s(stage + bytes / sizeof(float2), c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + roff, bytes,
+             bar);
+    return;
   }
-  return true;
+  mbar_expect_tx(bar, bytes);
+  if (!step_is_col(st.type)) {
+    const float2* base;
+    switch (st.type) {
+      case ST_REC_ROW0: base = c.ckpt + ((long long)k.b * c.ckpt_n + st.ckpt_slot) * plane; break;
+      case ST_REC_ROW:
+      case ST_REC_ROWL: base = c.work + (long long)k.b * plane; break;
+      case ST_ADJ_ROW:
+      case ST_ADJ_ROW0: base = c.lam + (long long)k.b * plane; break;
+      default: base = c.psi + (long long)k.b * plane; break;   // FWD_ROW, FWD_ROWN, SEED_ROW
+    }
+    bulk_g2s(stage, base + (long long)k.tile * c.rows * c.n, bytes, bar);
+  } else {
+    const int buf = st.type == ST_FWD_COL ? BUF_PSI : st.type == ST_REC_COL ? BUF_WORK : BUF_LAM;
+    for (int r0 = 0; r0 < c.n; r0 += c.box_rows)
+      tma_load_2d(stage + r0 * c.cols_w, &P.maps[k.cls][buf], k.tile * c.cols_w, k.b * c.n + r0, bar);
+  }
 }
 
 constexpr int kComputeWarps = kSchedThreads / 32;      // 8 compute warps
 constexpr int kBlockThreads = kSchedThreads + 32;       // + 1 producer warp
 constexpr int kFftBar = 2;                              // named barrier of the compute warps
 
+// ---------------------------------------------------------------------------
+// tile bodies
+// ---------------------------------------------------------------------------
 // Row tile, phase 1: this thread's E input words into registers.
 template <int N, int E>
-__device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, const float2* stage, float2 (&v)[E]) {
+__device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, int type, const float2* stage,
+                                         float2 (&v)[E]) {
   constexpr int T = N / E;
   const int rl = threadIdx.x / T, t = threadIdx.x - rl * T;
-  if (k.pass == 0) {
+  if (type == ST_FWD_ROW0) {
     // move_probe (propagation.py:263-276): roll psi0 by position - (n//2, n//2)
     const int row = k.tile * c.rows + rl;
     int sy = 0, sx = 0;
@@ -215,45 +328,131 @@ __device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, con
   }
 }
 
-// Row tile, phase 2: [inverse row FFT, scale], [* t_s, forward row FFT], store.
-template <int N, int E>
-__device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, float2 (&v)[E], float2* exch,
-                                            const float4* tw) {
+// Row tile, phase 2.  ttab holds t / (n n): the inverse transform's
+// normalisation rides on the transmission multiply; steps without an inverse
+// transform undo it, steps without a transmission apply it.  All these factors
+// are powers of two, so no rounding changes.
+template <int N, int E, bool GRAD, class Release>
+__device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, const Step& st, float2 (&v)[E],
+                                            float2* exch, const float4* tw, const float2* stage2,
+                                            const Release& release) {
   constexpr int T = N / E;
   constexpr int PADN = RowExchange<true>::padded(N);
   const int rl = threadIdx.x / T, t = threadIdx.x - rl * T;
   const int row = k.tile * c.rows + rl;
   const long long plane = (long long)N * N;
   const RowExchange<(T <= 32), kFftBar, kSchedThreads> xs{exch + rl * PADN};
-  // ttab holds t / (n n): the inverse transform's normalisation rides on the
-  // transmission multiply; the first pass (no inverse transform) undoes it
-  // and the last pass (no transmission) applies it.  All factors are powers
-  // of two, so this changes no rounding.
-  if (k.pass != 0) {
-    fft<N, E, true>(v, t, xs, tw);
-  } else {
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
-  }
-  if (k.pass == 2 * c.n_slices) {
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.scale);
-  }
-  if (k.pass < 2 * c.n_slices) {
+  const int type = st.type;
+  // offset of this row in V / ttab / grad; evaluated after the inverse
+  // transform so that it is not live across it
+  auto row_off = [&]() -> long long {
     const int d = c.draw ? c.draw[k.b] : 0;
-    const float2* trow =
-        c.ttab + (long long)d * c.ttab_draw_stride + (long long)(k.pass >> 1) * plane + (long long)row * N;
+    return (long long)d * c.vstride + (long long)st.slice * plane + (long long)row * N;
+  };
+
+  if constexpr (!GRAD) {
+    // plain forward: [inverse row FFT], then * t and row FFT, or the exit wave
+    if (type != ST_FWD_ROW0) fft<N, E, true>(v, t, xs, tw);
+    float2* prow = c.psi + (long long)k.b * plane + (long long)row * N;
+    if (type == ST_FWD_ROWN) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, cscale(v[e], c.scale));
+      return;
+    }
+    if (type == ST_FWD_ROW0) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
+    }
+    const float2* trow = c.ttab + row_off();
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
     fft<N, E, false>(v, t, xs, tw);
-  }
-  float2* prow = c.psi + (long long)k.b * plane + (long long)row * N;
 #pragma unroll
-  for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
+    for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
+    return;
+  }
+
+  // --- inverse row transform (unnormalised) of the previous column output
+  const bool has_ifft = type == ST_FWD_ROW || type == ST_FWD_ROWN || type == ST_REC_ROW || type == ST_REC_ROWL ||
+                        type == ST_ADJ_ROW || type == ST_ADJ_ROW0;
+  if (has_ifft) fft<N, E, true>(v, t, xs, tw);
+
+  if (type == ST_FWD_ROWN) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.scale);
+    float2* prow = c.psi + (long long)k.b * plane + (long long)row * N;
+#pragma unroll
+    for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
+    return;
+  }
+
+  if constexpr (GRAD) {
+    // snapshots of the (normalised) wave entering slice st.slice
+    if (st.ckpt_slot >= 0 && (type == ST_FWD_ROW0 || type == ST_FWD_ROW)) {
+      float2* sp = c.ckpt + ((long long)k.b * c.ckpt_n + st.ckpt_slot) * plane + (long long)row * N;
+      const float sc = type == ST_FWD_ROW0 ? 1.0f : c.scale;
+#pragma unroll
+      for (int e = 0; e < E; ++e) __stcg(sp + t + T * e, cscale(v[e], sc));
+    }
+    if (st.seg_slot >= 0 && (type == ST_FWD_ROW0 || type == ST_FWD_ROW || type == ST_REC_ROW0 ||
+                             type == ST_REC_ROW || type == ST_REC_ROWL)) {
+      float2* sp = c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + (long long)row * N;
+      const float sc = (type == ST_FWD_ROW0 || type == ST_REC_ROW0) ? 1.0f : c.scale;
+#pragma unroll
+      for (int e = 0; e < E; ++e) __stcg(sp + t + T * e, cscale(v[e], sc));
+    }
+    if (type == ST_REC_ROWL) return;
+    if (type == ST_ADJ_ROW || type == ST_ADJ_ROW0) {
+      // v = n^2 lambda_a.  a_s = psi_s t_s; dL/dV = 2 Re(conj(lambda_a) i a_s) dphi/dV,
+      // dphi/dV = kphase (E + E0 + V) inv_den / n; lambda_psi = conj(t_s) lambda_a
+      // psi_s: from the second stage (TMA) or straight from the segment buffer
+      const float2* prow = stage2 ? stage2 + rl * N
+                                  : c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + (long long)row * N;
+      const long long tro = row_off();
+      const float* vrow = c.V + tro;
+      const float2* trow = c.ttab + tro;
+      float* grow = c.grad + tro;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int x = t + T * e;
+        const float2 lam = cscale(v[e], c.scale);
+        const float2 tt = cscale(__ldg(trow + x), c.inv_scale);
+        const float2 as = cmul(stage2 ? prow[x] : __ldcg(prow + x), tt);
+        const float vv = __ldg(vrow + x);
+        const float dn = refr_minus_one(vv, c.ri_a, c.ri_inv_den);
+        const float dphidv = c.kphase * (c.e_plus_e0 + vv) * c.ri_inv_den / (1.0f + dn);
+        atomicAdd(grow + x, 2.0f * (lam.y * as.x - lam.x * as.y) * dphidv);
+        v[e] = cmulc(lam, tt);
+      }
+      release();   // both stages consumed
+      if (type == ST_ADJ_ROW0) return;
+      fft<N, E, false>(v, t, xs, tw);
+      float2* orow = c.lam + (long long)k.b * plane + (long long)row * N;
+#pragma unroll
+      for (int e = 0; e < E; ++e) __stcg(orow + t + T * e, v[e]);
+      return;
+    }
+  }
+
+  // --- transmission (forward / recompute rows) and forward row transform
+  if (type == ST_FWD_ROW0 || type == ST_REC_ROW0) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
+  }
+  if (type != ST_SEED_ROW) {
+    const float2* trow = c.ttab + row_off();
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
+  }
+  fft<N, E, false>(v, t, xs, tw);
+  float2* dst = (type == ST_SEED_ROW) ? c.lam : (type == ST_REC_ROW0 || type == ST_REC_ROW) ? c.work : c.psi;
+  float2* orow = dst + (long long)k.b * plane + (long long)row * N;
+#pragma unroll
+  for (int e = 0; e < E; ++e) __stcg(orow + t + T * e, v[e]);
 }
 
 template <int N, int E>
-__device__ __forceinline__ void col_load(const SchedClass& c, const float2* stage, float2 (&v)[E]) {
+__device__ __forceinline__ void col_load(const float2* stage, float2 (&v)[E]) {
   constexpr int T = N / E;
   constexpr int W = kSchedThreads / T;
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
@@ -261,26 +460,47 @@ __device__ __forceinline__ void col_load(const SchedClass& c, const float2* stag
   for (int e = 0; e < E; ++e) v[e] = stage[(t + T * e) * W + cc];
 }
 
-// Column tile: FFT, * H (hi + lo), [dp on the last slice], inverse FFT, store.
-template <int N, int E>
-__device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, float2 (&v)[E], float2* exch,
-                                            const float4* tw) {
+// Column tile: FFT, * H or conj(H) (hi + lo), [dp / adjoint seed], inverse FFT.
+template <int N, int E, bool GRAD>
+__device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, const Step& st, float2 (&v)[E],
+                                            float2* exch, const float4* tw) {
   constexpr int T = N / E;
   constexpr int W = kSchedThreads / T;
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
   const int col = k.tile * W + cc;
   const long long plane = (long long)N * N;
   const ColExchange<kFftBar, kSchedThreads> xs{exch, W, cc};
+  const int type = st.type;
   fft<N, E, false>(v, t, xs, tw);
-  const float4* hcol = c.Hq + col;
+  const int sx = (col + (N >> 1)) & (N - 1);
+  if constexpr (GRAD) {
+    if (type == ST_SEED_COL) {
+      // lambda seed: n^2 g Z with g = dL/d(dp) at the fftshifted position
+      const float* gp = c.g + (long long)k.b * plane;
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const float4 h = __ldg(hcol + (t + T * e) * N);
-    v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
+      for (int e = 0; e < E; ++e) {
+        const int sy = (t + T * e + (N >> 1)) & (N - 1);
+        v[e] = cscale(v[e], c.inv_scale * __ldg(gp + (long long)sy * N + sx));
+      }
+    }
   }
-  if (c.dp && (k.pass >> 1) == c.n_slices - 1) {
+  const float4* hcol = c.Hq + col;
+  const bool conj = GRAD && (type == ST_SEED_COL || type == ST_ADJ_COL);
+  if (conj) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const float4 h = __ldg(hcol + (t + T * e) * N);
+      v[e] = cmulc_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const float4 h = __ldg(hcol + (t + T * e) * N);
+      v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
+    }
+  }
+  if ((!GRAD || type == ST_FWD_COL) && c.dp && st.slice == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
-    const int sx = (col + (N >> 1)) & (N - 1);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int sy = (t + T * e + (N >> 1)) & (N - 1);
@@ -288,27 +508,15 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     }
   }
   fft<N, E, true>(v, t, xs, tw);
-  float2* pcol = c.psi + (long long)k.b * plane + col;
+  float2* dst = !GRAD || type == ST_FWD_COL ? c.psi : type == ST_REC_COL ? c.work : c.lam;
+  float2* pcol = dst + (long long)k.b * plane + col;
 #pragma unroll
   for (int e = 0; e < E; ++e) __stcg(pcol + (long long)(t + T * e) * N, v[e]);
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// bounded mbarrier wait; false if the limit expired
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit) {
-  long long spins = 0;
-  while (!mbar_try_wait(bar, phase)) {
-    if (++spins > limit) return false;
-  }
-  return true;
-}
-
 // Compute warps: take the published tile, pull it into registers, release the
 // stage, run the transforms, store, report completion.
-template <unsigned MASK, int E>
+template <unsigned MASK, int E, bool GRAD>
 __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage, float2* exch, const float4* tw_smem,
                                              uint64_t* full, uint64_t* empty, uint64_t* done_bar, const Task* s_task) {
   uint32_t fph = 0;
@@ -324,7 +532,7 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
     fph ^= 1u;
     const Task k = *s_task;
     if (!k.valid) return;
-    if (!task_ok(P, k, 1)) {
+    if (!task_ok<GRAD>(P, k, 1)) {
       __syncwarp();
       if (lane == 0) {
         mbar_arrive(empty);
@@ -334,18 +542,32 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
       continue;
     }
     const SchedClass& c = P.cls[k.cls];
+    const Step st = step_of<GRAD>(c, k.pass);
     const float4* tw = P.tw_in_smem ? tw_smem + c.tw_off : c.tw;
+    const bool col = step_is_col(st.type);
+    // adjoint rows with a second stage release the stages only after they
+    // have read psi_s from it
+    const bool late = GRAD && P.stage2 && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0);
+    const float2* st2 = late ? stage + kTileBytesFor(E) / sizeof(float2) : nullptr;
+    auto release = [&]() {
+      if (late) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty);
+      }
+    };
     float2 v[E];
-#define WAP_SCHED_CASE(N, BIT)                                  \
-    if constexpr ((MASK & BIT) != 0) {                            \
-      if (c.n == N) {                                             \
-        if (k.pass & 1) col_load<N, E>(c, stage, v);              \
-        else row_load<N, E>(c, k, stage, v);                      \
-        __syncwarp();                                             \
-        if (lane == 0) mbar_arrive(empty);                        \
-        if (k.pass & 1) col_compute<N, E>(c, k, v, exch, tw);     \
-        else row_compute<N, E>(c, k, v, exch, tw);                \
-      }                                                           \
+#define WAP_SCHED_CASE(N, BIT)                                            \
+    if constexpr ((MASK & BIT) != 0) {                                      \
+      if (c.n == N) {                                                       \
+        if (col) col_load<N, E>(stage, v);                                  \
+        else row_load<N, E>(c, k, st.type, stage, v);                       \
+        if (!late) {                                                        \
+          __syncwarp();                                                     \
+          if (lane == 0) mbar_arrive(empty);                                \
+        }                                                                   \
+        if (col) col_compute<N, E, GRAD>(c, k, st, v, exch, tw);            \
+        else row_compute<N, E, GRAD>(c, k, st, v, exch, tw, st2, release);  \
+      }                                                                     \
     }
     WAP_SCHED_CASE(128, 1u)
     WAP_SCHED_CASE(256, 2u)
@@ -361,13 +583,14 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
 // ---------------------------------------------------------------------------
 // the persistent kernel: 8 compute warps + 1 producer warp
 // ---------------------------------------------------------------------------
-template <unsigned MASK, int E>
+template <unsigned MASK, int E, bool GRAD>
 __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(const __grid_constant__ SchedParams P) {
   extern __shared__ __align__(1024) unsigned char sched_smem[];
   float2* stage = reinterpret_cast<float2*>(sched_smem);
   constexpr int kTile = kTileBytesFor(E), kExch = kExchBytesFor(E);
-  float2* exch = reinterpret_cast<float2*>(sched_smem + kTile);
-  float4* tw_smem = reinterpret_cast<float4*>(sched_smem + kTile + kExch);
+  const int stages = (GRAD && P.stage2) ? 2 : 1;
+  float2* exch = reinterpret_cast<float2*>(sched_smem + stages * kTile);
+  float4* tw_smem = reinterpret_cast<float4*>(sched_smem + stages * kTile + kExch);
   __shared__ __align__(8) uint64_t full, empty, done_bar[2];
   __shared__ Task s_task;
 
@@ -387,7 +610,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   __syncthreads();
 
   if (threadIdx.x < kSchedThreads) {
-    compute_loop<MASK, E>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
+    compute_loop<MASK, E, GRAD>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
     return;
   }
 
@@ -413,7 +636,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
     return out;
   };
   auto need_of = [&](const Task& k) -> int {
-    return k.pass == P.stall_pass ? 0x7fffffff : tiles_before(P.cls[k.cls], k.pass);
+    return k.pass == P.stall_pass ? 0x7fffffff : step_of<GRAD>(P.cls[k.cls], k.pass).prefix;
   };
   auto counter_of = [&](const Task& k) -> const int* { return P.done + P.cls[k.cls].done_off + k.b; };
   // Block until the task's inputs are complete (bounded).  Only called while
@@ -435,39 +658,28 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
     fence_proxy_async();
     return true;
   };
-  auto tile_bytes = [&](const Task& k) -> uint32_t {
-    const SchedClass& c = P.cls[k.cls];
-    if (k.pass == 0) return 0;
-    return (k.pass & 1) ? (uint32_t)(c.n * c.cols_w * 8) : (uint32_t)(c.rows * c.n * 8);
-  };
-  // publish a task (or the stop sentinel) to the compute warps
+  // publish a task (or the stop sentinel) to the compute warps: exactly one
+  // arrival per phase on `full` (count 1) - issue_load's arrive.expect_tx for
+  // tiles with a TMA load, a plain arrive otherwise
+  uint32_t fph = 0;            // parity of the next full-barrier phase to complete
+  bool load_out = false;       // the latest published item carried a TMA load
   auto publish = [&](const Task& k0) {
     Task k = k0;
-    if (k.valid && !task_ok(P, k, 2)) k.valid = 0;
+    if (k.valid && !task_ok<GRAD>(P, k, 2)) k.valid = 0;
     s_task = k;
-    // exactly one arrival per phase on `full` (count 1): issue_load's
-    // arrive.expect_tx for tiles with a TMA load, a plain arrive otherwise
-    const uint32_t bytes = k.valid ? tile_bytes(k) : 0;
-    if (bytes) {
-      issue_load(P, k, stage, &full);
-    } else {
-      mbar_arrive(&full);
-    }
+    const uint32_t bytes = k.valid ? tile_bytes(P.cls[k.cls], step_of<GRAD>(P.cls[k.cls], k.pass).type) : 0u;
+    load_out = bytes != 0;
+    if (bytes) issue_load<GRAD>(P, k, stage, &full);
+    else mbar_arrive(&full);
+    fph ^= 1u;
   };
   auto fail_wait = [&]() { atomicCAS(P.status, 0, WAP_ERR_TIMEOUT); };
 
   uint32_t eph = 0, dph[2] = {0, 0};
   uint32_t tiles_signalled = 0;
-  uint32_t fph = 0;            // parity of the next full-barrier phase to complete
-  bool load_out = false;       // the latest published item carried a TMA load
-  auto publish_track = [&](const Task& kk) {
-    load_out = kk.valid && tile_bytes(kk) != 0;
-    publish(kk);
-    fph ^= 1u;
-  };
   Task k = claim();
   if (k.valid && !wait_ready(k)) k.valid = 0;
-  publish_track(k);
+  publish(k);
   while (k.valid) {
     Task kn = claim();
     bool issued = false;
@@ -476,7 +688,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
       if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
       eph ^= 1u;
       fence_proxy_async();
-      publish_track(kn);
+      publish(kn);
       issued = true;
     }
     // completion of k: every compute warp has stored its part.  The compute
@@ -495,7 +707,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
       if (kn.valid && !wait_ready(kn)) kn.valid = 0;
       if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
       eph ^= 1u;
-      publish_track(kn);   // kn or the stop sentinel
+      publish(kn);   // kn or the stop sentinel
     }
     k = kn;
   }
@@ -515,29 +727,40 @@ typedef void (*ScanKernel)(const SchedParams);
 
 // kernel instances by elements per thread and the set of grid sizes they
 // contain (bit 0: 128, 1: 256, 2: 512, 3: 1024); other sets use the
-// all-sizes instance
+// all-sizes instance.  Gradient instances hold one size each.
 template <int E>
-static ScanKernel pick_scan_kernel_e(unsigned mask) {
+static ScanKernel pick_fwd_e(unsigned mask) {
   switch (mask) {
-    case 1u: return scan_kernel<1u, E>;
-    case 2u: return scan_kernel<2u, E>;
-    case 4u: return scan_kernel<4u, E>;
-    case 8u: return scan_kernel<8u, E>;
-    case 6u: return scan_kernel<6u, E>;
-    default: return scan_kernel<15u, E>;
+    case 1u: return scan_kernel<1u, E, false>;
+    case 2u: return scan_kernel<2u, E, false>;
+    case 4u: return scan_kernel<4u, E, false>;
+    case 8u: return scan_kernel<8u, E, false>;
+    case 6u: return scan_kernel<6u, E, false>;
+    default: return scan_kernel<15u, E, false>;
   }
 }
-static ScanKernel pick_scan_kernel(unsigned mask, int e) {
-  return e == 8 ? pick_scan_kernel_e<8>(mask) : pick_scan_kernel_e<16>(mask);
+static ScanKernel pick_grad(unsigned mask) {
+  switch (mask) {
+    case 1u: return scan_kernel<1u, 16, true>;
+    case 2u: return scan_kernel<2u, 16, true>;
+    case 4u: return scan_kernel<4u, 16, true>;
+    default: return scan_kernel<8u, 16, true>;
+  }
 }
 
 struct wap_scan {
   ScanKernel kernel = nullptr;
+  bool grad = false;
   int e = 16;
   int device = 0;
   int n_classes = 0;
   SchedParams params{};
-  SchedDesc* d_desc = nullptr;
+  SchedDesc* d_desc = nullptr;      // forward descriptors
+  SchedDesc* d_desc_bwd = nullptr;  // backward descriptors (gradient scans)
+  int n_desc = 0, n_desc_bwd = 0;
+  long long n_tickets = 0, n_tickets_bwd = 0;
+  Step* d_steps = nullptr;          // forward chains of all classes, back to back
+  Step* d_steps_bwd = nullptr;      // backward chain (gradient scans: one class)
   unsigned long long* d_ticket = nullptr;
   int* d_done = nullptr;
   int* d_status = nullptr;
@@ -545,13 +768,16 @@ struct wap_scan {
   int total_probes = 0;
   int grid = 0;
   size_t smem = 0;
+  int grid_bwd = 0;                 // backward launch: two staging buffers
+  size_t smem_bwd = 0;
+  int ckpt_every = 0;
   std::vector<float4*> d_tw;
   std::vector<float2*> d_ttab;
   std::vector<float4*> d_hq;
+  std::vector<void*> d_extra;       // gradient buffers
   std::vector<size_t> ttab_elems;
   std::vector<wap_scan_class> cls;
   std::vector<Physics> phys;
-  long long n_tickets = 0;
 };
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -569,6 +795,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 static void scan_free(wap_scan* s) {
   if (!s) return;
   cudaFree(s->d_desc);
+  cudaFree(s->d_desc_bwd);
+  cudaFree(s->d_steps);
+  cudaFree(s->d_steps_bwd);
   cudaFree(s->d_ticket);
   cudaFree(s->d_done);
   cudaFree(s->d_status);
@@ -576,46 +805,141 @@ static void scan_free(wap_scan* s) {
   for (auto p : s->d_tw) cudaFree(p);
   for (auto p : s->d_ttab) cudaFree(p);
   for (auto p : s->d_hq) cudaFree(p);
+  for (auto p : s->d_extra) cudaFree(p);
   delete s;
 }
 
 static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n == 1024; }
 
-extern "C" {
+// column-tile tensor map over (B n rows) x (n columns) of 8-byte elements
+static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map, void* base, int n, int n_probes,
+                      int cols_w, int box_rows) {
+  cuuint64_t gdim[2] = {(cuuint64_t)n, (cuuint64_t)n_probes * n};
+  cuuint64_t gstride[1] = {(cuuint64_t)n * 8};
+  cuuint32_t box[2] = {(cuuint32_t)cols_w, (cuuint32_t)box_rows};
+  cuuint32_t estride[2] = {1, 1};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_INT64, 2, base, gdim, gstride, box, estride,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(WAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return WAP_OK;
+}
 
-int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes) {
-  clear_error();
-  if (!out) return fail(WAP_ERR_ARG, "scan pointer is NULL");
-  *out = nullptr;
-  if (n_classes < 1 || n_classes > kMaxClasses || !classes)
-    return fail(WAP_ERR_ARG, "n_classes must be in [1, %d]", kMaxClasses);
+// Forward chain of one class: steps 0..2N (rows even, columns odd).  With
+// ckpt_every > 0 the rows also store checkpoints (every k-th slice) and the
+// waves of the last k-slice segment.
+static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, std::vector<Step>& out) {
+  const int N = n_slices;
+  const int k = ckpt_every;
+  const int nck = k > 0 ? (N + k - 1) / k : 0;
+  const int last0 = k > 0 ? (nck - 1) * k : N;
+  int prefix = 0;
+  for (int p = 0; p <= 2 * N; ++p) {
+    Step st{};
+    st.slice = p >> 1;
+    st.ckpt_slot = -1;
+    st.seg_slot = -1;
+    if (p & 1) {
+      st.type = ST_FWD_COL;
+    } else if (p == 2 * N) {
+      st.type = ST_FWD_ROWN;
+    } else {
+      st.type = p == 0 ? ST_FWD_ROW0 : ST_FWD_ROW;
+      if (k > 0 && st.slice % k == 0) st.ckpt_slot = st.slice / k;
+      if (k > 0 && st.slice >= last0) st.seg_slot = st.slice - last0;
+    }
+    st.seg0 = k > 0 ? (st.slice / k) * k : 0;
+    st.prefix = prefix;
+    prefix += (p & 1) ? sc.col_tiles : sc.row_tiles;
+    out.push_back(st);
+  }
+}
+
+// Backward chain: seed, then per segment (last first) recompute + adjoint.
+static void backward_steps(const SchedClass& sc, int n_slices, int k, std::vector<Step>& out) {
+  const int N = n_slices;
+  const int nck = (N + k - 1) / k;
+  int prefix = 0;
+  auto push = [&](int type, int slice, int seg0, int ckpt_slot, int seg_slot) {
+    Step st{type, slice, seg0, ckpt_slot, seg_slot, prefix};
+    prefix += step_is_col(type) ? sc.col_tiles : sc.row_tiles;
+    out.push_back(st);
+  };
+  push(ST_SEED_ROW, N - 1, 0, -1, -1);
+  push(ST_SEED_COL, N - 1, 0, -1, -1);
+  for (int j = nck - 1; j >= 0; --j) {
+    const int s0 = j * k, s1 = std::min(s0 + k, N);
+    if (j != nck - 1) {
+      push(ST_REC_ROW0, s0, s0, j, 0);
+      if (s1 - s0 > 1) {
+        push(ST_REC_COL, s0, s0, -1, -1);
+        for (int s = s0 + 1; s < s1 - 1; ++s) {
+          push(ST_REC_ROW, s, s0, -1, s - s0);
+          push(ST_REC_COL, s, s0, -1, -1);
+        }
+        push(ST_REC_ROWL, s1 - 1, s0, -1, s1 - 1 - s0);
+      }
+    }
+    for (int s = s1 - 1; s >= s0; --s) {
+      push(s == 0 ? ST_ADJ_ROW0 : ST_ADJ_ROW, s, s0, -1, s - s0);
+      if (s > 0) push(ST_ADJ_COL, s, s0, -1, -1);
+    }
+  }
+}
+
+// Descriptors: groups of G probes walk through a class's chain.
+static void build_desc(const std::vector<Step>& steps, int ci, int n_probes, int G, long long& ticket,
+                       const SchedClass& sc, std::vector<SchedDesc>& out) {
+  for (int b0 = 0; b0 < n_probes; b0 += G) {
+    const int nb = std::min(G, n_probes - b0);
+    for (size_t p = 0; p < steps.size(); ++p) {
+      SchedDesc d;
+      d.base = ticket;
+      d.cls = ci;
+      d.pass = (int)p;
+      d.b0 = b0;
+      d.nprobes = nb;
+      d.tiles = step_is_col(steps[p].type) ? sc.col_tiles : sc.row_tiles;
+      out.push_back(d);
+      ticket += (long long)nb * d.tiles;
+    }
+  }
+}
+
+template <class T>
+static int upload(T** dst, const std::vector<T>& src, const char* what) {
+  cudaError_t e = cudaMalloc(dst, std::max<size_t>(1, src.size()) * sizeof(T));
+  if (e == cudaSuccess && !src.empty()) e = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? WAP_OK : cuda_fail(e, what);
+}
+
+// Shared set-up of forward scans (ckpt_every = 0) and gradient scans.
+static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes, int ckpt_every) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = get_encode();
   if (!encode) return fail(WAP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  wap_scan* s = new wap_scan();
   cudaGetDevice(&s->device);
   s->n_classes = n_classes;
   s->cls.assign(classes, classes + n_classes);
+  s->grad = ckpt_every > 0;
+  s->ckpt_every = ckpt_every;
   cudaError_t e;
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-  // elements per thread of the scheduler's transforms
+  // elements per thread of the scheduler's transforms (16; 8 for A/B timing)
   int E = 16;
-  if (const char* ov = getenv("WAP_SCHED_E")) {   // debugging / A-B timing only
-    if (!strcmp(ov, "8")) E = 8;
+  if (const char* ov = getenv("WAP_SCHED_E")) {
+    if (!strcmp(ov, "8") && !s->grad) E = 8;
   }
   s->e = E;
   unsigned mask = 0;
   int tw_total = 0;
   for (int ci = 0; ci < n_classes; ++ci) {
     const int n = classes[ci].n;
-    if (!sched_size_ok(n)) {
-      scan_free(s);
-      return fail(WAP_ERR_UNSUPPORTED, "scan grids must be 128, 256, 512 or 1024 (got %d)", n);
-    }
+    if (!sched_size_ok(n)) return fail(WAP_ERR_UNSUPPORTED, "scan grids must be 128, 256, 512 or 1024 (got %d)", n);
     mask |= n == 128 ? 1u : n == 256 ? 2u : n == 512 ? 4u : 8u;
     tw_total += make_plan_shape(n, E).tw_size();
   }
-  s->kernel = pick_scan_kernel(mask, E);
+  s->kernel = s->grad ? pick_grad(mask) : (E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask));
   // Keep the twiddles in shared memory only when they fit next to the stage
   // and exchange buffers without lowering the CTAs per SM (3 for E = 16,
   // 4 for E = 8).
@@ -627,27 +951,33 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
     if (!strcmp(ov, "global")) s->params.tw_in_smem = 0;
   }
   s->smem = base_smem + (s->params.tw_in_smem ? (size_t)tw_total * sizeof(float4) : 0);
-  if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem)) != cudaSuccess) {
-    scan_free(s);
+  if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem)) != cudaSuccess)
     return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
-  }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kernel, kBlockThreads, s->smem);
-  if (per_sm < 1) {
-    scan_free(s);
-    return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
-  }
+  if (per_sm < 1) return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
   s->grid = sms * per_sm;
+  if (s->grad) {
+    // the backward stages psi_s next to lambda: one more tile of shared memory
+    s->smem_bwd = s->smem + kTileBytesFor(E);
+    int per_sm_bwd = 0;
+    if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_bwd)) !=
+        cudaSuccess)
+      return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bwd, s->kernel, kBlockThreads, s->smem_bwd);
+    s->grid_bwd = sms * std::max(1, per_sm_bwd);
+  }
   int tw_off = 0;
 
-  std::vector<SchedDesc> desc;
-  long long ticket = 0;
+  std::vector<SchedDesc> desc, desc_bwd;
+  std::vector<Step> steps_all, steps_bwd_all;
+  std::vector<size_t> step_off;
+  long long ticket = 0, ticket_bwd = 0;
   int done_off = 0;
+  int rc;
   for (int ci = 0; ci < n_classes; ++ci) {
     const wap_scan_class& c = classes[ci];
-    if (c.n_slices < 1 || c.n_draws < 1 || c.n_probes < 1 || !c.V || !c.psi0 || !c.H || !c.exit) {
-      scan_free(s);
+    if (c.n_slices < 1 || c.n_draws < 1 || c.n_probes < 1 || !c.V || !c.psi0 || !c.H || !c.exit)
       return fail(WAP_ERR_ARG, "scan class %d: bad sizes or NULL V/psi0/H/exit", ci);
-    }
     const int n = c.n, T = n / E;
     SchedClass& sc = s->params.cls[ci];
     sc.n = n;
@@ -664,94 +994,97 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
     sc.psi0 = reinterpret_cast<const float2*>(c.psi0);
     sc.positions = c.positions;
     sc.draw = c.draw;
-    float4* dhq = nullptr;
-    if ((e = cudaMalloc(&dhq, (size_t)n * n * sizeof(float4))) != cudaSuccess) {
-      scan_free(s);
-      return cuda_fail(e, "cudaMalloc(interleaved H)");
-    }
-    s->d_hq.push_back(dhq);
-    sc.Hq = dhq;
+    sc.V = c.V;
     sc.dp = c.dp;
+    sc.vstride = (long long)c.n_slices * n * n;
     sc.scale = (float)(1.0 / ((double)n * n));
     sc.inv_scale = (float)((double)n * n);
-    sc.ttab_draw_stride = (long long)c.n_slices * n * n;
-    // twiddles
+    const Physics ph = physics(c.energy, c.dz);
+    s->phys.push_back(ph);
+    sc.ri_a = (float)ph.ri_a;
+    sc.ri_inv_den = (float)ph.ri_inv_den;
+    sc.kphase = (float)ph.kphase;
+    sc.e_plus_e0 = (float)ph.e_plus_e0;
+    float4* dhq = nullptr;
+    if ((e = cudaMalloc(&dhq, (size_t)n * n * sizeof(float4))) != cudaSuccess)
+      return cuda_fail(e, "cudaMalloc(interleaved H)");
+    s->d_hq.push_back(dhq);
+    sc.Hq = dhq;
     std::vector<float4> h = twiddle_table(n, E);
     float4* dtw = nullptr;
-    if ((e = cudaMalloc(&dtw, h.size() * sizeof(float4))) != cudaSuccess ||
-        (e = cudaMemcpy(dtw, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice)) != cudaSuccess) {
-      cudaFree(dtw);
-      scan_free(s);
-      return cuda_fail(e, "twiddle upload");
-    }
+    if ((rc = upload(&dtw, h, "twiddle upload")) != WAP_OK) return rc;
     s->d_tw.push_back(dtw);
     sc.tw = dtw;
     sc.tw_off = tw_off;
     sc.tw_len = (int)h.size();
     tw_off += sc.tw_len;
-    // transmission table
     const size_t tt = (size_t)c.n_draws * c.n_slices * n * n;
     float2* dtt = nullptr;
-    if ((e = cudaMalloc(&dtt, tt * sizeof(float2))) != cudaSuccess) {
-      scan_free(s);
-      return cuda_fail(e, "cudaMalloc(transmission table)");
-    }
+    if ((e = cudaMalloc(&dtt, tt * sizeof(float2))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(transmission table)");
     s->d_ttab.push_back(dtt);
     s->ttab_elems.push_back(tt);
     sc.ttab = dtt;
-    s->phys.push_back(physics(c.energy, c.dz));
-    // column-tile tensor map: 2D (n columns x B n rows) of 8-byte elements
-    cuuint64_t gdim[2] = {(cuuint64_t)n, (cuuint64_t)c.n_probes * n};
-    cuuint64_t gstride[1] = {(cuuint64_t)n * 8};
-    cuuint32_t box[2] = {(cuuint32_t)sc.cols_w, (cuuint32_t)sc.box_rows};
-    cuuint32_t estride[2] = {1, 1};
-    CUresult r = encode(&s->params.maps[ci], CU_TENSOR_MAP_DATA_TYPE_INT64, 2, c.exit, gdim, gstride, box, estride,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-      scan_free(s);
-      return fail(WAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for class %d", (int)r, ci);
-    }
-    // pass descriptors: groups of G probes walk through all passes
-    int G = c.group;
-    if (G <= 0) {
-      // enough tiles per pass to cover the resident CTAs twice, and a group
-      // footprint of ~32 MB so that the group's waves stay in L2
-      const int tiles = sc.row_tiles;
-      G = std::max(1, (2 * s->grid + tiles - 1) / tiles);
-      const int l2_cap = std::max(1, (int)((32ll << 20) / ((long long)n * n * 8)));
-      G = std::min(std::max(G, 1), std::max(l2_cap, 1));
-    }
-    G = std::min(G, c.n_probes);
-    for (int b0 = 0; b0 < c.n_probes; b0 += G) {
-      const int nb = std::min(G, c.n_probes - b0);
-      for (int p = 0; p <= 2 * c.n_slices; ++p) {
-        SchedDesc d;
-        d.base = ticket;
-        d.cls = ci;
-        d.pass = p;
-        d.b0 = b0;
-        d.nprobes = nb;
-        d.tiles = (p & 1) ? sc.col_tiles : sc.row_tiles;
-        desc.push_back(d);
-        ticket += (long long)nb * d.tiles;
+    if (s->grad) {
+      const int k = ckpt_every;
+      sc.ckpt_n = (c.n_slices + k - 1) / k;
+      sc.seg_n = k;
+      const size_t plane = (size_t)n * n, B = (size_t)c.n_probes;
+      const size_t sizes[4] = {B * plane * 8, B * plane * 8, B * k * plane * 8, B * sc.ckpt_n * plane * 8};
+      float2** dsts[4] = {&sc.lam, &sc.work, &sc.seg, &sc.ckpt};
+      for (int i = 0; i < 4; ++i) {
+        void* p = nullptr;
+        if ((e = cudaMalloc(&p, sizes[i])) != cudaSuccess) return cuda_fail(e, "cudaMalloc(gradient buffers)");
+        s->d_extra.push_back(p);
+        *dsts[i] = reinterpret_cast<float2*>(p);
       }
     }
+    if ((rc = encode_map(encode, &s->params.maps[ci][BUF_PSI], c.exit, n, c.n_probes, sc.cols_w, sc.box_rows)))
+      return rc;
+    if (s->grad) {
+      if ((rc = encode_map(encode, &s->params.maps[ci][BUF_LAM], sc.lam, n, c.n_probes, sc.cols_w, sc.box_rows)))
+        return rc;
+      if ((rc = encode_map(encode, &s->params.maps[ci][BUF_WORK], sc.work, n, c.n_probes, sc.cols_w, sc.box_rows)))
+        return rc;
+    }
+    // chains and descriptors: groups of G probes walk through all steps
+    std::vector<Step> steps, steps_bwd;
+    forward_steps(sc, c.n_slices, ckpt_every, steps);
+    if (s->grad) backward_steps(sc, c.n_slices, ckpt_every, steps_bwd);
+    int G = c.group;
+    if (G <= 0) {
+      // enough tiles per step to cover the resident CTAs twice (a group's
+      // steps are a dependency chain, so this is the parallelism available),
+      // and no more, so that the group's waves stay in L2
+      G = std::max(1, (2 * s->grid + sc.row_tiles - 1) / sc.row_tiles);
+    }
+    G = std::min(G, c.n_probes);
+    build_desc(steps, ci, c.n_probes, G, ticket, sc, desc);
+    if (s->grad) build_desc(steps_bwd, ci, c.n_probes, G, ticket_bwd, sc, desc_bwd);
+    step_off.push_back(steps_all.size());
+    steps_all.insert(steps_all.end(), steps.begin(), steps.end());
+    steps_bwd_all.insert(steps_bwd_all.end(), steps_bwd.begin(), steps_bwd.end());
     done_off += c.n_probes;
   }
   s->n_tickets = ticket;
+  s->n_tickets_bwd = ticket_bwd;
   s->total_probes = done_off;
-  if ((e = cudaMalloc(&s->d_desc, desc.size() * sizeof(SchedDesc))) != cudaSuccess ||
-      (e = cudaMemcpy(s->d_desc, desc.data(), desc.size() * sizeof(SchedDesc), cudaMemcpyHostToDevice)) != cudaSuccess ||
-      (e = cudaMalloc(&s->d_ticket, sizeof(unsigned long long))) != cudaSuccess ||
+  s->n_desc = (int)desc.size();
+  s->n_desc_bwd = (int)desc_bwd.size();
+  if ((rc = upload(&s->d_desc, desc, "scan descriptors")) || (rc = upload(&s->d_steps, steps_all, "scan steps")))
+    return rc;
+  if (s->grad && ((rc = upload(&s->d_desc_bwd, desc_bwd, "scan descriptors")) ||
+                  (rc = upload(&s->d_steps_bwd, steps_bwd_all, "scan steps"))))
+    return rc;
+  for (int ci = 0; ci < n_classes; ++ci) s->params.cls[ci].steps = s->d_steps + step_off[ci];
+  if ((e = cudaMalloc(&s->d_ticket, sizeof(unsigned long long))) != cudaSuccess ||
       (e = cudaMalloc(&s->d_done, (size_t)done_off * sizeof(int))) != cudaSuccess ||
-      (e = cudaMalloc(&s->d_status, sizeof(int))) != cudaSuccess) {
-    scan_free(s);
+      (e = cudaMalloc(&s->d_status, sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&s->d_debug, 8 * sizeof(int))) != cudaSuccess)
     return cuda_fail(e, "scan allocation");
-  }
   cudaMemset(s->d_status, 0, sizeof(int));
+  cudaMemset(s->d_debug, 0, 8 * sizeof(int));
   s->params.desc = s->d_desc;
-  s->params.n_desc = (int)desc.size();
+  s->params.n_desc = s->n_desc;
   s->params.n_classes = n_classes;
   s->params.total = ticket;
   s->params.ticket = s->d_ticket;
@@ -760,41 +1093,47 @@ int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes
   s->params.spin_limit = kSpinLimit;
   s->params.stall_pass = -1;
   s->params.checks = 0;
-  if ((e = cudaMalloc(&s->d_debug, 8 * sizeof(int))) != cudaSuccess) {
-    scan_free(s);
-    return cuda_fail(e, "scan allocation");
-  }
-  cudaMemset(s->d_debug, 0, 8 * sizeof(int));
   s->params.debug = s->d_debug;
-  *out = s;
   return WAP_OK;
 }
 
-int wap_scan_run(wap_scan* s, void* stream) {
-  clear_error();
-  if (!s) return fail(WAP_ERR_ARG, "scan is NULL");
-  cudaStream_t st = (cudaStream_t)stream;
+// issue resets, per-class tables and the persistent kernel for one chain
+static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(s->d_ticket, 0, sizeof(unsigned long long), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(s->d_done, 0, (size_t)s->total_probes * sizeof(int), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(s->d_status, 0, sizeof(int), st)) != cudaSuccess)
     return cuda_fail(e, "scan reset");
-  for (int ci = 0; ci < s->n_classes; ++ci) {
-    const Physics& ph = s->phys[ci];
-    const long long n4 = (long long)s->ttab_elems[ci] / 4;
-    const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
-    count_launch();
-    trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
-        s->cls[ci].V, s->d_ttab[ci], n4, (float)ph.ri_a, (float)ph.ri_inv_den, (float)ph.kphase,
-        s->params.cls[ci].scale);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
-    prof_end(tok, st, 12.0 * (double)s->ttab_elems[ci]);
-    const long long nn = (long long)s->cls[ci].n * s->cls[ci].n;
-    count_launch();
-    interleave_h_kernel<<<(unsigned)std::min<long long>((nn + 255) / 256, 148LL * 8), 256, 0, st>>>(
-        reinterpret_cast<const float2*>(s->cls[ci].H), reinterpret_cast<const float2*>(s->cls[ci].H_lo),
-        s->d_hq[ci], nn);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "interleave_h_kernel");
+  SchedParams params = s->params;
+  params.stage2 = 0;
+  int grid = s->grid;
+  size_t smem = s->smem;
+  if (backward) {
+    params.stage2 = 1;
+    grid = s->grid_bwd;
+    smem = s->smem_bwd;
+    params.desc = s->d_desc_bwd;
+    params.n_desc = s->n_desc_bwd;
+    params.total = s->n_tickets_bwd;
+    params.cls[0].steps = s->d_steps_bwd;   // gradient scans hold one class
+  } else {
+    for (int ci = 0; ci < s->n_classes; ++ci) {
+      const Physics& ph = s->phys[ci];
+      const long long n4 = (long long)s->ttab_elems[ci] / 4;
+      const ProfToken tok = prof_begin(WAP_KIND_TRANS, st);
+      count_launch();
+      trans_table_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
+          s->cls[ci].V, s->d_ttab[ci], n4, (float)ph.ri_a, (float)ph.ri_inv_den, (float)ph.kphase,
+          s->params.cls[ci].scale);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "trans_table_kernel");
+      prof_end(tok, st, 12.0 * (double)s->ttab_elems[ci]);
+      const long long nn = (long long)s->cls[ci].n * s->cls[ci].n;
+      count_launch();
+      interleave_h_kernel<<<(unsigned)std::min<long long>((nn + 255) / 256, 148LL * 8), 256, 0, st>>>(
+          reinterpret_cast<const float2*>(s->cls[ci].H), reinterpret_cast<const float2*>(s->cls[ci].H_lo),
+          s->d_hq[ci], nn);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "interleave_h_kernel");
+    }
   }
   // algorithmic bytes of a slice step: wave in 8 + wave out 8 + potential 4
   // per pixel (the two passes' intermediate round trip is not counted)
@@ -805,10 +1144,96 @@ int wap_scan_run(wap_scan* s, void* stream) {
   }
   const ProfToken tok = prof_begin(WAP_KIND_SCHED, st);
   count_launch();
-  s->kernel<<<s->grid, kBlockThreads, s->smem, st>>>(s->params);
+  s->kernel<<<grid, kBlockThreads, smem, st>>>(params);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scan_kernel");
   prof_end(tok, st, bytes);
   return WAP_OK;
+}
+
+extern "C" {
+
+int wap_scan_create(wap_scan** out, int n_classes, const wap_scan_class* classes) {
+  clear_error();
+  if (!out) return fail(WAP_ERR_ARG, "scan pointer is NULL");
+  *out = nullptr;
+  if (n_classes < 1 || n_classes > kMaxClasses || !classes)
+    return fail(WAP_ERR_ARG, "n_classes must be in [1, %d]", kMaxClasses);
+  wap_scan* s = new wap_scan();
+  const int rc = scan_setup(s, n_classes, classes, 0);
+  if (rc != WAP_OK) {
+    scan_free(s);
+    return rc;
+  }
+  *out = s;
+  return WAP_OK;
+}
+
+int wap_scan_grad_create(wap_scan** out, const wap_scan_class* cls, int ckpt_every) {
+  clear_error();
+  if (!out || !cls) return fail(WAP_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  if (ckpt_every < 1) return fail(WAP_ERR_ARG, "ckpt_every must be >= 1");
+  if (!cls->dp) return fail(WAP_ERR_ARG, "the gradient scan needs a dp buffer");
+  wap_scan* s = new wap_scan();
+  const int rc = scan_setup(s, 1, cls, std::min(ckpt_every, cls->n_slices));
+  if (rc != WAP_OK) {
+    scan_free(s);
+    return rc;
+  }
+  *out = s;
+  return WAP_OK;
+}
+
+// Re-point a scan at new buffers with the same shapes (no device allocation):
+// pointers of every class and the wave's column-tile tensor map are replaced.
+int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
+  clear_error();
+  if (!s || !classes) return fail(WAP_ERR_ARG, "NULL argument");
+  if (n_classes != s->n_classes) return fail(WAP_ERR_ARG, "scan has %d classes, got %d", s->n_classes, n_classes);
+  PFN_cuTensorMapEncodeTiled_v12000 encode = get_encode();
+  if (!encode) return fail(WAP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  for (int ci = 0; ci < n_classes; ++ci) {
+    const wap_scan_class& c = classes[ci];
+    const wap_scan_class& o = s->cls[ci];
+    if (c.n != o.n || c.n_slices != o.n_slices || c.n_draws != o.n_draws || c.n_probes != o.n_probes)
+      return fail(WAP_ERR_ARG, "scan class %d: shapes differ from the ones the scan was created for", ci);
+    if (!c.V || !c.psi0 || !c.H || !c.exit) return fail(WAP_ERR_ARG, "scan class %d: NULL V/psi0/H/exit", ci);
+    if (s->grad && !c.dp) return fail(WAP_ERR_ARG, "the gradient scan needs a dp buffer");
+    SchedClass& sc = s->params.cls[ci];
+    CUtensorMap map;
+    int rc = encode_map(encode, &map, c.exit, c.n, c.n_probes, sc.cols_w, sc.box_rows);
+    if (rc) return rc;
+    s->params.maps[ci][BUF_PSI] = map;
+    sc.psi = reinterpret_cast<float2*>(c.exit);
+    sc.psi0 = reinterpret_cast<const float2*>(c.psi0);
+    sc.positions = c.positions;
+    sc.draw = c.draw;
+    sc.V = c.V;
+    sc.dp = c.dp;
+    s->cls[ci] = c;
+    s->phys[ci] = physics(c.energy, c.dz);
+    const Physics& ph = s->phys[ci];
+    sc.ri_a = (float)ph.ri_a;
+    sc.ri_inv_den = (float)ph.ri_inv_den;
+    sc.kphase = (float)ph.kphase;
+    sc.e_plus_e0 = (float)ph.e_plus_e0;
+  }
+  return WAP_OK;
+}
+
+int wap_scan_run(wap_scan* s, void* stream) {
+  clear_error();
+  if (!s) return fail(WAP_ERR_ARG, "scan is NULL");
+  return scan_launch(s, false, (cudaStream_t)stream);
+}
+
+int wap_scan_grad_backward(wap_scan* s, const float* grad_dp, float* grad_V, void* stream) {
+  clear_error();
+  if (!s || !grad_dp || !grad_V) return fail(WAP_ERR_ARG, "NULL argument");
+  if (!s->grad) return fail(WAP_ERR_ARG, "scan was not created for gradients");
+  s->params.cls[0].g = grad_dp;
+  s->params.cls[0].grad = grad_V;
+  return scan_launch(s, true, (cudaStream_t)stream);
 }
 
 int wap_scan_status(wap_scan* s, int* status) {

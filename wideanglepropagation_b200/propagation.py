@@ -293,6 +293,36 @@ def _prepare(potential, probe, positions, draw, dev):
     return V, psi, per_probe, pos, dr, B, n_slices, ny, nx, batched
 
 
+SCAN_SIZES = (128, 256, 512, 1024)
+SCAN_MIN_PROBES = 8
+_scans: dict = {}
+_scans_lock = threading.Lock()
+
+
+def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp):
+    """Run a batched forward through the persistent scheduler (cached per shape)."""
+    D, N, n, _ = V.shape
+    B = exit_wave.shape[0]
+    dev = torch.cuda.current_device()
+    key = (dev, n, N, D, B)
+    cls = (_lib.ScanClass * 1)()
+    cls[0] = _lib.ScanClass(n, N, D, B, V.data_ptr(), dr.data_ptr() if dr is not None else None, psi.data_ptr(),
+                            pos.data_ptr() if pos is not None else None, H.data_ptr(),
+                            H_lo.data_ptr() if H_lo is not None else None, float(dz), float(energy),
+                            exit_wave.data_ptr(), dp.data_ptr(), 0)
+    L = _lib.lib()
+    arr = ctypes.cast(cls, ctypes.c_void_p)
+    with _scans_lock:
+        h = _scans.get(key)
+        if h is None:
+            h = ctypes.c_void_p()
+            _lib.check(L.wap_scan_create(ctypes.byref(h), 1, arr))
+            _scans[key] = h
+        else:
+            _lib.check(L.wap_scan_bind(h, 1, arr))
+        _lib.check(L.wap_scan_run(h, _stream()))
+
+
 def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, *,
                         return_wavefronts: bool = True, positions=None, draw=None):
     """Fresnel / angular-spectrum multislice (propagation.py:305-352).
@@ -309,9 +339,16 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     H, H_lo = split_transfer(prop_kernel, dev)
     if H.shape != (ny, nx):
         raise ValueError(f"prop_kernel shape {tuple(H.shape)} does not match grid {(ny, nx)}")
-    plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
     exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
     dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+    if (not return_wavefronts and ny == nx and ny in SCAN_SIZES and B >= SCAN_MIN_PROBES
+            and not per_probe):
+        # many probes of one shared probe: the persistent batched scheduler
+        _scan_run(V, psi, pos, dr, H, H_lo, slice_thickness, energy, exit_wave, dp)
+        if not batched:
+            exit_wave, dp = exit_wave[0], dp[0]
+        return exit_wave, dp, None
+    plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
