@@ -95,8 +95,9 @@ struct Step {
   int type;
   int slice;
   int seg0;       // first slice of the step's checkpoint segment
-  int ckpt_slot;  // forward rows: checkpoint slot written (-1: none); REC_ROW0: slot read
-  int seg_slot;   // forward/recompute rows: segment slot written; ADJ rows: slot read
+  int ckpt_slot;  // forward rows: checkpoint slot written (-1: none); REC_ROW0 and the
+                  // ADJ row of a segment's first slice: checkpoint slot read
+  int seg_slot;   // forward/recompute rows: segment slot written; other ADJ rows: slot read
   int prefix;     // tiles of all earlier steps of the probe
 };
 
@@ -122,14 +123,21 @@ struct SchedClass {
   float2* seg;                  // (B, k, n, n) waves of the current segment
   float2* ckpt;                 // (B, nck, n, n) checkpoints
   int ckpt_n, seg_n;            // slots per probe
+  int ckpt_k;                   // gradient scans: checkpoint every ckpt_k slices (0: none)
+  int seg_first;                // first slice of the last segment (kept by the forward)
   const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp
-  float* grad;                  // (draws, N, n, n) dL/dV, accumulated
+  float* grad;                  // (draws, N, n, n) probe sums of Re(conj(lambda_a) i a_s)
   float ri_a, ri_inv_den, kphase, e_plus_e0;
   const float4* tw;             // twiddles for (n, E) in global memory
   int tw_off, tw_len;           // their place in the shared-memory copy
   float scale;                  // 1 / (n n)  (also folded into ttab)
   float inv_scale;              // n n
 };
+
+// Where adjoint rows read psi_s (the wave entering the slice) from:
+constexpr int kPsiGlobal = 0;   // global loads inside the tile body
+constexpr int kPsiStage2 = 1;   // a second staging buffer, loaded with lambda
+constexpr int kPsiSplit = 2;    // the one stage, refilled once lambda is in registers
 
 struct SchedDesc {
   long long base;   // first ticket
@@ -150,7 +158,7 @@ struct alignas(64) SchedParams {
   int stall_pass;                  // test hook: tiles of this step wait forever (-1: off)
   int checks;                      // validate every task before use (debug)
   int tw_in_smem;                  // twiddles copied to shared memory (else read via L1)
-  int stage2;                      // a second staging buffer: adjoint rows get psi_s by TMA too
+  int stage2;                      // how adjoint rows get psi_s: kPsiGlobal / kPsiStage2 / kPsiSplit
   int* debug;                      // [code, cls, step, b, tile, extra] of the first bad task
 };
 
@@ -223,6 +231,11 @@ __device__ __forceinline__ Step forward_step(const SchedClass& c, int pass) {
   st.seg0 = 0;
   st.ckpt_slot = -1;
   st.seg_slot = -1;
+  if (c.ckpt_k > 0 && !(pass & 1) && st.slice < c.n_slices) {
+    // gradient scans: checkpoints every ckpt_k slices, the last segment whole
+    if (st.slice % c.ckpt_k == 0) st.ckpt_slot = st.slice / c.ckpt_k;
+    if (st.slice > c.seg_first) st.seg_slot = st.slice - c.seg_first;   // seg_first: its checkpoint
+  }
   st.prefix = ((pass + 1) >> 1) * c.row_tiles + (pass >> 1) * c.col_tiles;
   return st;
 }
@@ -260,6 +273,14 @@ __device__ __forceinline__ uint32_t tile_bytes(const SchedClass& c, int type) {
   return step_is_col(type) ? (uint32_t)(c.n * c.cols_w * 8) : (uint32_t)(c.rows * c.n * 8);
 }
 
+// psi_s of an adjoint row (whole plane of probe b): the checkpoint for a
+// segment's first slice, else the segment buffer
+__device__ __forceinline__ const float2* adj_psi(const SchedClass& c, const Step& st, int b) {
+  const long long plane = (long long)c.n * c.n;
+  return st.ckpt_slot >= 0 ? c.ckpt + ((long long)b * c.ckpt_n + st.ckpt_slot) * plane
+                           : c.seg + ((long long)b * c.seg_n + st.seg_slot) * plane;
+}
+
 // Issue the TMA load of a task's input tile into `stage` (one thread).  This
 // is the single arrival of the phase on `bar`: arrive.expect_tx(tile bytes),
 // completed by the copy.  Not called for tasks that load directly.
@@ -269,13 +290,12 @@ __device__ __forceinline__ void issue_load(const SchedParams& P, const Task& k, 
   const Step st = step_of<GRAD>(c, k.pass);
   const long long plane = (long long)c.n * c.n;
   const uint32_t bytes = tile_bytes(c, st.type);
-  if (GRAD && P.stage2 && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0)) {
+  if (GRAD && P.stage2 == kPsiStage2 && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0)) {
     // lambda rows into the stage, the same rows of psi_s into the second stage
     mbar_expect_tx(bar, 2 * bytes);
     const long long roff = (long long)k.tile * c.rows * c.n;
     bulk_g2s(stage, c.lam + (long long)k.b * plane + roff, bytes, bar);
-    bulk_g2s(stage + bytes / sizeof(float2), c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + roff, bytes,
-             bar);
+    bulk_g2s(stage + bytes / sizeof(float2), adj_psi(c, st, k.b) + roff, bytes, bar);
     return;
   }
   mbar_expect_tx(bar, bytes);
@@ -331,11 +351,13 @@ __device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, int
 // Row tile, phase 2.  ttab holds t / (n n): the inverse transform's
 // normalisation rides on the transmission multiply; steps without an inverse
 // transform undo it, steps without a transmission apply it.  All these factors
-// are powers of two, so no rounding changes.
-template <int N, int E, bool GRAD, class Release>
+// are powers of two, so no rounding changes.  The forward instance (!GRAD)
+// runs the forward chain - with checkpoint / segment snapshots in gradient
+// scans - and the gradient instance runs the backward chain.
+template <int N, int E, bool GRAD, class Acquire, class Release>
 __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, const Step& st, float2 (&v)[E],
                                             float2* exch, const float4* tw, const float2* stage2,
-                                            const Release& release) {
+                                            const Acquire& acquire, const Release& release) {
   constexpr int T = N / E;
   constexpr int PADN = RowExchange<true>::padded(N);
   const int rl = threadIdx.x / T, t = threadIdx.x - rl * T;
@@ -349,9 +371,16 @@ __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, 
     const int d = c.draw ? c.draw[k.b] : 0;
     return (long long)d * c.vstride + (long long)st.slice * plane + (long long)row * N;
   };
+  // normalised wave entering slice st.slice into a snapshot slot
+  auto snapshot = [&](float2* base, int slot, int slots, bool unnormalised) {
+    float2* sp = base + ((long long)k.b * slots + slot) * plane + (long long)row * N;
+    const float sc = unnormalised ? c.scale : 1.0f;
+#pragma unroll
+    for (int e = 0; e < E; ++e) __stcg(sp + t + T * e, cscale(v[e], sc));
+  };
 
   if constexpr (!GRAD) {
-    // plain forward: [inverse row FFT], then * t and row FFT, or the exit wave
+    // forward: [inverse row FFT], then * t and row FFT, or the exit wave
     if (type != ST_FWD_ROW0) fft<N, E, true>(v, t, xs, tw);
     float2* prow = c.psi + (long long)k.b * plane + (long long)row * N;
     if (type == ST_FWD_ROWN) {
@@ -359,6 +388,8 @@ __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, 
       for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, cscale(v[e], c.scale));
       return;
     }
+    if (st.ckpt_slot >= 0) snapshot(c.ckpt, st.ckpt_slot, c.ckpt_n, type != ST_FWD_ROW0);
+    if (st.seg_slot >= 0) snapshot(c.seg, st.seg_slot, c.seg_n, type != ST_FWD_ROW0);
     if (type == ST_FWD_ROW0) {
 #pragma unroll
       for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
@@ -370,61 +401,34 @@ __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, 
 #pragma unroll
     for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
     return;
-  }
-
-  // --- inverse row transform (unnormalised) of the previous column output
-  const bool has_ifft = type == ST_FWD_ROW || type == ST_FWD_ROWN || type == ST_REC_ROW || type == ST_REC_ROWL ||
-                        type == ST_ADJ_ROW || type == ST_ADJ_ROW0;
-  if (has_ifft) fft<N, E, true>(v, t, xs, tw);
-
-  if (type == ST_FWD_ROWN) {
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.scale);
-    float2* prow = c.psi + (long long)k.b * plane + (long long)row * N;
-#pragma unroll
-    for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
-    return;
-  }
-
-  if constexpr (GRAD) {
-    // snapshots of the (normalised) wave entering slice st.slice
-    if (st.ckpt_slot >= 0 && (type == ST_FWD_ROW0 || type == ST_FWD_ROW)) {
-      float2* sp = c.ckpt + ((long long)k.b * c.ckpt_n + st.ckpt_slot) * plane + (long long)row * N;
-      const float sc = type == ST_FWD_ROW0 ? 1.0f : c.scale;
-#pragma unroll
-      for (int e = 0; e < E; ++e) __stcg(sp + t + T * e, cscale(v[e], sc));
-    }
-    if (st.seg_slot >= 0 && (type == ST_FWD_ROW0 || type == ST_FWD_ROW || type == ST_REC_ROW0 ||
-                             type == ST_REC_ROW || type == ST_REC_ROWL)) {
-      float2* sp = c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + (long long)row * N;
-      const float sc = (type == ST_FWD_ROW0 || type == ST_REC_ROW0) ? 1.0f : c.scale;
-#pragma unroll
-      for (int e = 0; e < E; ++e) __stcg(sp + t + T * e, cscale(v[e], sc));
-    }
+  } else {
+    // --- inverse row transform (unnormalised) of the previous column output
+    if (type != ST_REC_ROW0 && type != ST_SEED_ROW) fft<N, E, true>(v, t, xs, tw);
+    // recompute rows keep the wave entering their slice for the adjoint sweep
+    if (st.seg_slot >= 0 && (type == ST_REC_ROW0 || type == ST_REC_ROW || type == ST_REC_ROWL))
+      snapshot(c.seg, st.seg_slot, c.seg_n, type != ST_REC_ROW0);
     if (type == ST_REC_ROWL) return;
     if (type == ST_ADJ_ROW || type == ST_ADJ_ROW0) {
-      // v = n^2 lambda_a.  a_s = psi_s t_s; dL/dV = 2 Re(conj(lambda_a) i a_s) dphi/dV,
-      // dphi/dV = kphase (E + E0 + V) inv_den / n; lambda_psi = conj(t_s) lambda_a
-      // psi_s: from the second stage (TMA) or straight from the segment buffer
-      const float2* prow = stage2 ? stage2 + rl * N
-                                  : c.seg + ((long long)k.b * c.seg_n + st.seg_slot) * plane + (long long)row * N;
+      // v = n^2 lambda_a.  a_s = psi_s t_s; dL/dV = 2 Re(conj(lambda_a) i a_s) dphi/dV.
+      // dphi/dV depends on V alone, so the probes' sum of Re(conj(lambda_a) i a_s)
+      // is accumulated here and scaled by 2 dphi/dV once per voxel after the
+      // sweep (grad_finalize_kernel).  lambda_psi = conj(t_s) lambda_a.
+      // psi_s: from the stage (TMA) or straight from the segment buffer.
+      const float2* prow = stage2 ? stage2 + rl * N : adj_psi(c, st, k.b) + (long long)row * N;
       const long long tro = row_off();
-      const float* vrow = c.V + tro;
       const float2* trow = c.ttab + tro;
       float* grow = c.grad + tro;
+      acquire();   // psi_s has landed in the stage (split mode)
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int x = t + T * e;
         const float2 lam = cscale(v[e], c.scale);
         const float2 tt = cscale(__ldg(trow + x), c.inv_scale);
         const float2 as = cmul(stage2 ? prow[x] : __ldcg(prow + x), tt);
-        const float vv = __ldg(vrow + x);
-        const float dn = refr_minus_one(vv, c.ri_a, c.ri_inv_den);
-        const float dphidv = c.kphase * (c.e_plus_e0 + vv) * c.ri_inv_den / (1.0f + dn);
-        atomicAdd(grow + x, 2.0f * (lam.y * as.x - lam.x * as.y) * dphidv);
+        atomicAdd(grow + x, lam.y * as.x - lam.x * as.y);
         v[e] = cmulc(lam, tt);
       }
-      release();   // both stages consumed
+      release();   // psi_s consumed
       if (type == ST_ADJ_ROW0) return;
       fft<N, E, false>(v, t, xs, tw);
       float2* orow = c.lam + (long long)k.b * plane + (long long)row * N;
@@ -432,23 +436,22 @@ __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, 
       for (int e = 0; e < E; ++e) __stcg(orow + t + T * e, v[e]);
       return;
     }
-  }
-
-  // --- transmission (forward / recompute rows) and forward row transform
-  if (type == ST_FWD_ROW0 || type == ST_REC_ROW0) {
+    // recompute rows: * t and forward row transform; the seed row: transform only
+    if (type == ST_REC_ROW0) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
-  }
-  if (type != ST_SEED_ROW) {
-    const float2* trow = c.ttab + row_off();
+      for (int e = 0; e < E; ++e) v[e] = cscale(v[e], c.inv_scale);
+    }
+    if (type != ST_SEED_ROW) {
+      const float2* trow = c.ttab + row_off();
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
-  }
-  fft<N, E, false>(v, t, xs, tw);
-  float2* dst = (type == ST_SEED_ROW) ? c.lam : (type == ST_REC_ROW0 || type == ST_REC_ROW) ? c.work : c.psi;
-  float2* orow = dst + (long long)k.b * plane + (long long)row * N;
+      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
+    }
+    fft<N, E, false>(v, t, xs, tw);
+    float2* dst = (type == ST_SEED_ROW) ? c.lam : c.work;
+    float2* orow = dst + (long long)k.b * plane + (long long)row * N;
 #pragma unroll
-  for (int e = 0; e < E; ++e) __stcg(orow + t + T * e, v[e]);
+    for (int e = 0; e < E; ++e) __stcg(orow + t + T * e, v[e]);
+  }
 }
 
 template <int N, int E>
@@ -499,7 +502,7 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
     }
   }
-  if ((!GRAD || type == ST_FWD_COL) && c.dp && st.slice == c.n_slices - 1) {
+  if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -508,7 +511,7 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     }
   }
   fft<N, E, true>(v, t, xs, tw);
-  float2* dst = !GRAD || type == ST_FWD_COL ? c.psi : type == ST_REC_COL ? c.work : c.lam;
+  float2* dst = !GRAD ? c.psi : type == ST_REC_COL ? c.work : c.lam;
   float2* pcol = dst + (long long)k.b * plane + col;
 #pragma unroll
   for (int e = 0; e < E; ++e) __stcg(pcol + (long long)(t + T * e) * N, v[e]);
@@ -545,12 +548,24 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
     const Step st = step_of<GRAD>(c, k.pass);
     const float4* tw = P.tw_in_smem ? tw_smem + c.tw_off : c.tw;
     const bool col = step_is_col(st.type);
-    // adjoint rows with a second stage release the stages only after they
-    // have read psi_s from it
-    const bool late = GRAD && P.stage2 && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0);
-    const float2* st2 = late ? stage + kTileBytesFor(E) / sizeof(float2) : nullptr;
+    // Adjoint rows read psi_s next to lambda.  kPsiStage2: both arrive
+    // together (second stage), released after psi_s is read.  kPsiSplit:
+    // lambda is released as usual, then the producer refills the same stage
+    // with psi_s - a second phase of `full` that lands during the inverse row
+    // transform - released after psi_s is read.
+    const bool adj = GRAD && (st.type == ST_ADJ_ROW || st.type == ST_ADJ_ROW0);
+    const bool late = adj && P.stage2 == kPsiStage2;
+    const bool split = adj && P.stage2 == kPsiSplit;
+    const float2* st2 = late ? stage + kTileBytesFor(E) / sizeof(float2) : split ? stage : nullptr;
+    auto acquire = [&]() {
+      if (split) {
+        for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit); ++round)
+          atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
+        fph ^= 1u;
+      }
+    };
     auto release = [&]() {
-      if (late) {
+      if (late || split) {
         __syncwarp();
         if (lane == 0) mbar_arrive(empty);
       }
@@ -566,7 +581,7 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
           if (lane == 0) mbar_arrive(empty);                                \
         }                                                                   \
         if (col) col_compute<N, E, GRAD>(c, k, st, v, exch, tw);            \
-        else row_compute<N, E, GRAD>(c, k, st, v, exch, tw, st2, release);  \
+        else row_compute<N, E, GRAD>(c, k, st, v, exch, tw, st2, acquire, release); \
       }                                                                     \
     }
     WAP_SCHED_CASE(128, 1u)
@@ -588,7 +603,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   extern __shared__ __align__(1024) unsigned char sched_smem[];
   float2* stage = reinterpret_cast<float2*>(sched_smem);
   constexpr int kTile = kTileBytesFor(E), kExch = kExchBytesFor(E);
-  const int stages = (GRAD && P.stage2) ? 2 : 1;
+  const int stages = (GRAD && P.stage2 == kPsiStage2) ? 2 : 1;
   float2* exch = reinterpret_cast<float2*>(sched_smem + stages * kTile);
   float4* tw_smem = reinterpret_cast<float4*>(sched_smem + stages * kTile + kExch);
   __shared__ __align__(8) uint64_t full, empty, done_bar[2];
@@ -661,21 +676,34 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   // publish a task (or the stop sentinel) to the compute warps: exactly one
   // arrival per phase on `full` (count 1) - issue_load's arrive.expect_tx for
   // tiles with a TMA load, a plain arrive otherwise
+  auto fail_wait = [&]() { atomicCAS(P.status, 0, WAP_ERR_TIMEOUT); };
+  uint32_t eph = 0, dph[2] = {0, 0};
   uint32_t fph = 0;            // parity of the next full-barrier phase to complete
   bool load_out = false;       // the latest published item carried a TMA load
   auto publish = [&](const Task& k0) {
     Task k = k0;
     if (k.valid && !task_ok<GRAD>(P, k, 2)) k.valid = 0;
     s_task = k;
-    const uint32_t bytes = k.valid ? tile_bytes(P.cls[k.cls], step_of<GRAD>(P.cls[k.cls], k.pass).type) : 0u;
+    const SchedClass& c = P.cls[k.cls];
+    const int type = k.valid ? step_of<GRAD>(c, k.pass).type : -1;
+    const uint32_t bytes = k.valid ? tile_bytes(c, type) : 0u;
     load_out = bytes != 0;
     if (bytes) issue_load<GRAD>(P, k, stage, &full);
     else mbar_arrive(&full);
     fph ^= 1u;
+    if (GRAD && P.stage2 == kPsiSplit && (type == ST_ADJ_ROW || type == ST_ADJ_ROW0)) {
+      // second phase of the same tile: once every compute warp holds lambda,
+      // refill the stage with the matching rows of psi_s
+      if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
+      eph ^= 1u;
+      fence_proxy_async();
+      const Step st = step_of<GRAD>(c, k.pass);
+      mbar_expect_tx(&full, bytes);
+      bulk_g2s(stage, adj_psi(c, st, k.b) + (long long)k.tile * c.rows * c.n, bytes, &full);
+      fph ^= 1u;
+    }
   };
-  auto fail_wait = [&]() { atomicCAS(P.status, 0, WAP_ERR_TIMEOUT); };
 
-  uint32_t eph = 0, dph[2] = {0, 0};
   uint32_t tiles_signalled = 0;
   Task k = claim();
   if (k.valid && !wait_ready(k)) k.valid = 0;
@@ -716,6 +744,30 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   if (load_out && *(volatile int*)P.status != 0) mbar_wait(&full, fph ^ 1u, P.spin_limit);
 }
 
+// dL/dV += 2 dphi/dV(V) S for every voxel, S being the probes' sum of
+// Re(conj(lambda_a) i a_s) from the adjoint sweep.  phi = kphase (n(V) - 1)
+// with n(V) of propagation.py:66-81, so dphi/dV = kphase (E + E0 + V)
+// inv_den / n(V).
+static __global__ void __launch_bounds__(256) grad_finalize_kernel(const float* __restrict__ V,
+                                                            const float* __restrict__ S, float* __restrict__ grad,
+                                                            long long n4, float a, float inv_den, float kphase,
+                                                            float e_plus_e0) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(V) + i);
+    const float4 sm = __ldcs(reinterpret_cast<const float4*>(S) + i);
+    float4 g = reinterpret_cast<float4*>(grad)[i];
+    auto term = [&](float vv, float ss) {
+      const float dn = refr_minus_one(vv, a, inv_den);
+      return 2.0f * ss * (kphase * (e_plus_e0 + vv) * inv_den / (1.0f + dn));
+    };
+    g.x += term(v.x, sm.x);
+    g.y += term(v.y, sm.y);
+    g.z += term(v.z, sm.z);
+    g.w += term(v.w, sm.w);
+    reinterpret_cast<float4*>(grad)[i] = g;
+  }
+}
+
 }  // namespace wap
 
 // ---------------------------------------------------------------------------
@@ -749,7 +801,8 @@ static ScanKernel pick_grad(unsigned mask) {
 }
 
 struct wap_scan {
-  ScanKernel kernel = nullptr;
+  ScanKernel kernel = nullptr;       // forward chains (gradient scans: with snapshots)
+  ScanKernel kernel_bwd = nullptr;   // backward chain of gradient scans
   bool grad = false;
   int e = 16;
   int device = 0;
@@ -768,8 +821,10 @@ struct wap_scan {
   int total_probes = 0;
   int grid = 0;
   size_t smem = 0;
-  int grid_bwd = 0;                 // backward launch: two staging buffers
+  int grid_bwd = 0;                 // backward launch (two staging buffers with kPsiStage2)
   size_t smem_bwd = 0;
+  int psi_mode = kPsiSplit;         // how the backward's adjoint rows get psi_s
+  float* d_gsum = nullptr;          // (draws, N, n, n) probe sums of the adjoint sweep
   int ckpt_every = 0;
   std::vector<float4*> d_tw;
   std::vector<float2*> d_ttab;
@@ -806,6 +861,7 @@ static void scan_free(wap_scan* s) {
   for (auto p : s->d_ttab) cudaFree(p);
   for (auto p : s->d_hq) cudaFree(p);
   for (auto p : s->d_extra) cudaFree(p);
+  cudaFree(s->d_gsum);
   delete s;
 }
 
@@ -827,7 +883,8 @@ static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map
 
 // Forward chain of one class: steps 0..2N (rows even, columns odd).  With
 // ckpt_every > 0 the rows also store checkpoints (every k-th slice) and the
-// waves of the last k-slice segment.
+// waves of the last k-slice segment after its first slice (whose wave is its
+// checkpoint).
 static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, std::vector<Step>& out) {
   const int N = n_slices;
   const int k = ckpt_every;
@@ -846,7 +903,7 @@ static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, st
     } else {
       st.type = p == 0 ? ST_FWD_ROW0 : ST_FWD_ROW;
       if (k > 0 && st.slice % k == 0) st.ckpt_slot = st.slice / k;
-      if (k > 0 && st.slice >= last0) st.seg_slot = st.slice - last0;
+      if (k > 0 && st.slice > last0) st.seg_slot = st.slice - last0;
     }
     st.seg0 = k > 0 ? (st.slice / k) * k : 0;
     st.prefix = prefix;
@@ -856,6 +913,9 @@ static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, st
 }
 
 // Backward chain: seed, then per segment (last first) recompute + adjoint.
+// The recompute starts from the segment's checkpoint and keeps the waves
+// entering slices s0+1 .. s1-1; the adjoint row of slice s0 reads the
+// checkpoint itself (one-slice segments need no recompute at all).
 static void backward_steps(const SchedClass& sc, int n_slices, int k, std::vector<Step>& out) {
   const int N = n_slices;
   const int nck = (N + k - 1) / k;
@@ -869,19 +929,19 @@ static void backward_steps(const SchedClass& sc, int n_slices, int k, std::vecto
   push(ST_SEED_COL, N - 1, 0, -1, -1);
   for (int j = nck - 1; j >= 0; --j) {
     const int s0 = j * k, s1 = std::min(s0 + k, N);
-    if (j != nck - 1) {
-      push(ST_REC_ROW0, s0, s0, j, 0);
-      if (s1 - s0 > 1) {
-        push(ST_REC_COL, s0, s0, -1, -1);
-        for (int s = s0 + 1; s < s1 - 1; ++s) {
-          push(ST_REC_ROW, s, s0, -1, s - s0);
-          push(ST_REC_COL, s, s0, -1, -1);
-        }
-        push(ST_REC_ROWL, s1 - 1, s0, -1, s1 - 1 - s0);
+    if (j != nck - 1 && s1 - s0 > 1) {
+      push(ST_REC_ROW0, s0, s0, j, -1);
+      push(ST_REC_COL, s0, s0, -1, -1);
+      for (int s = s0 + 1; s < s1 - 1; ++s) {
+        push(ST_REC_ROW, s, s0, -1, s - s0);
+        push(ST_REC_COL, s, s0, -1, -1);
       }
+      push(ST_REC_ROWL, s1 - 1, s0, -1, s1 - 1 - s0);
     }
     for (int s = s1 - 1; s >= s0; --s) {
-      push(s == 0 ? ST_ADJ_ROW0 : ST_ADJ_ROW, s, s0, -1, s - s0);
+      const int type = s == 0 ? ST_ADJ_ROW0 : ST_ADJ_ROW;
+      if (s == s0) push(type, s, s0, j, -1);   // psi_s0 is checkpoint j
+      else push(type, s, s0, -1, s - s0);
       if (s > 0) push(ST_ADJ_COL, s, s0, -1, -1);
     }
   }
@@ -939,7 +999,8 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     mask |= n == 128 ? 1u : n == 256 ? 2u : n == 512 ? 4u : 8u;
     tw_total += make_plan_shape(n, E).tw_size();
   }
-  s->kernel = s->grad ? pick_grad(mask) : (E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask));
+  s->kernel = E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask);
+  if (s->grad) s->kernel_bwd = pick_grad(mask);
   // Keep the twiddles in shared memory only when they fit next to the stage
   // and exchange buffers without lowering the CTAs per SM (3 for E = 16,
   // 4 for E = 8).
@@ -957,14 +1018,19 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   if (per_sm < 1) return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
   s->grid = sms * per_sm;
   if (s->grad) {
-    // the backward stages psi_s next to lambda: one more tile of shared memory
-    s->smem_bwd = s->smem + kTileBytesFor(E);
+    // kPsiStage2 stages psi_s next to lambda: one more tile of shared memory
+    if (const char* ov = getenv("WAP_SCHED_PSI")) {   // A/B timing only
+      const int m = atoi(ov);
+      if (m >= kPsiGlobal && m <= kPsiSplit) s->psi_mode = m;
+    }
+    s->smem_bwd = s->smem + (s->psi_mode == kPsiStage2 ? kTileBytesFor(E) : 0);
     int per_sm_bwd = 0;
-    if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_bwd)) !=
+    if ((e = cudaFuncSetAttribute(s->kernel_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_bwd)) !=
         cudaSuccess)
       return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bwd, s->kernel, kBlockThreads, s->smem_bwd);
-    s->grid_bwd = sms * std::max(1, per_sm_bwd);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bwd, s->kernel_bwd, kBlockThreads, s->smem_bwd);
+    if (per_sm_bwd < 1) return fail(WAP_ERR_CUDA, "scan_kernel (backward) does not fit on an SM");
+    s->grid_bwd = sms * per_sm_bwd;
   }
   int tw_off = 0;
 
@@ -1028,6 +1094,8 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
       const int k = ckpt_every;
       sc.ckpt_n = (c.n_slices + k - 1) / k;
       sc.seg_n = k;
+      sc.ckpt_k = k;
+      sc.seg_first = (sc.ckpt_n - 1) * k;
       const size_t plane = (size_t)n * n, B = (size_t)c.n_probes;
       const size_t sizes[4] = {B * plane * 8, B * plane * 8, B * k * plane * 8, B * sc.ckpt_n * plane * 8};
       float2** dsts[4] = {&sc.lam, &sc.work, &sc.seg, &sc.ckpt};
@@ -1037,6 +1105,8 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
         s->d_extra.push_back(p);
         *dsts[i] = reinterpret_cast<float2*>(p);
       }
+      if ((e = cudaMalloc(&s->d_gsum, tt * sizeof(float))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(gradient sums)");
     }
     if ((rc = encode_map(encode, &s->params.maps[ci][BUF_PSI], c.exit, n, c.n_probes, sc.cols_w, sc.box_rows)))
       return rc;
@@ -1051,11 +1121,15 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     forward_steps(sc, c.n_slices, ckpt_every, steps);
     if (s->grad) backward_steps(sc, c.n_slices, ckpt_every, steps_bwd);
     int G = c.group;
+    if (const char* ov = getenv("WAP_SCHED_GROUP")) {   // A/B timing only
+      if (G <= 0) G = atoi(ov);
+    }
     if (G <= 0) {
-      // enough tiles per step to cover the resident CTAs twice (a group's
-      // steps are a dependency chain, so this is the parallelism available),
-      // and no more, so that the group's waves stay in L2
-      G = std::max(1, (2 * s->grid + sc.row_tiles - 1) / sc.row_tiles);
+      // enough tiles per step to cover the resident CTAs four times (a
+      // group's steps are a dependency chain, so this is the parallelism
+      // available), and no more, so that the group's waves stay in L2: about
+      // 4 x 444 tiles x 32 KB = 56 MB for every grid size on a 148-SM part
+      G = std::max(1, (4 * s->grid + sc.row_tiles - 1) / sc.row_tiles);
     }
     G = std::min(G, c.n_probes);
     build_desc(steps, ci, c.n_probes, G, ticket, sc, desc);
@@ -1109,7 +1183,10 @@ static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   int grid = s->grid;
   size_t smem = s->smem;
   if (backward) {
-    params.stage2 = 1;
+    params.stage2 = s->psi_mode;
+    params.cls[0].grad = s->d_gsum;
+    if ((e = cudaMemsetAsync(s->d_gsum, 0, s->ttab_elems[0] * sizeof(float), st)) != cudaSuccess)
+      return cuda_fail(e, "gradient sums reset");
     grid = s->grid_bwd;
     smem = s->smem_bwd;
     params.desc = s->d_desc_bwd;
@@ -1144,9 +1221,18 @@ static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   }
   const ProfToken tok = prof_begin(WAP_KIND_SCHED, st);
   count_launch();
-  s->kernel<<<grid, kBlockThreads, smem, st>>>(params);
+  (backward ? s->kernel_bwd : s->kernel)<<<grid, kBlockThreads, smem, st>>>(params);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scan_kernel");
   prof_end(tok, st, bytes);
+  if (backward) {
+    const Physics& ph = s->phys[0];
+    const long long n4 = (long long)s->ttab_elems[0] / 4;
+    count_launch();
+    grad_finalize_kernel<<<(unsigned)std::min<long long>((n4 + 255) / 256, 148LL * 16), 256, 0, st>>>(
+        s->cls[0].V, s->d_gsum, s->params.cls[0].grad, n4, (float)ph.ri_a, (float)ph.ri_inv_den, (float)ph.kphase,
+        (float)ph.e_plus_e0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "grad_finalize_kernel");
+  }
   return WAP_OK;
 }
 
