@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="tiny workload (testing the harness)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/grad/err/cpu sections")
     ap.add_argument("--profile-grad", action="store_true",
-                    help="gradient case for ncu captures: 64 probes 256^2 x 16 slices, checkpoint every 4, one "
-                         "forward + backward through the persistent scheduler")
+                    help="gradient case for ncu captures: the 512^2 x 64-slice inverse problem on a 4x4 probe "
+                         "raster (16 probes), checkpoint every 8, two forward + backward steps through the "
+                         "persistent scheduler")
     ap.add_argument("--mode", default="persistent", choices=["persistent", "batched", "graph"],
                     help="batched execution mode timed as the headline")
     ap.add_argument("--profile-case", action="store_true",
@@ -165,7 +166,7 @@ def profile_grad():
     import torch
     import wideanglepropagation_b200 as wap
     from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
-    w = wap.synthetic.inverse_problem(0, n=256, n_slices=16, n_side=8)
+    w = wap.synthetic.inverse_problem(0, n=512, n_slices=64, n_side=4)
     dev = torch.device("cuda", 0)
     H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
     probe = torch.as_tensor(w.probe).to(dev)
@@ -175,7 +176,7 @@ def profile_grad():
     V = torch.zeros_like(Vt, requires_grad=True)
     for _ in range(2):
         V.grad = None
-        _, dp = simulate_fresnel_as_differentiable(V, probe, H, w.dz, w.energy, positions=pos, ckpt_every=4)
+        _, dp = simulate_fresnel_as_differentiable(V, probe, H, w.dz, w.energy, positions=pos, ckpt_every=8)
         ((dp - target) ** 2).sum().backward()
     torch.cuda.synchronize()
     print(json.dumps({"profile_grad": "ok", "grad_norm": float(V.grad.norm())}))

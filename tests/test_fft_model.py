@@ -1,7 +1,7 @@
 """NumPy model of the per-thread Stockham schedule in csrc/wap_fft.cuh.
 
 Thread t holds x[t + T e]; stage s (radix R, span L) twiddles slot q + (E/R) j
-by W_{LR}^{jk} read from the [j][k] table at tw_offset(s) + j L + k, runs a
+by W_{LR}^{jk} read from the table of rows j = 1..R-1 at tw_offset(s) + (j-1) L + k, runs a
 radix-R DFT and scatters y_m to (b - k) R + k + m L.  The model uses the same
 plan arithmetic and table layout and must reproduce numpy.fft exactly (to
 rounding) for every size and elements-per-thread the kernels instantiate.
@@ -22,10 +22,10 @@ def twiddle_table(N, E):
     for s in range(1, len(radices)):
         R = radices[s]
         offs.append(off)
-        for j in range(R):
+        for j in range(1, R):
             for k in range(L):
                 tab.append(np.exp(-2j * np.pi * ((j * k) % (L * R)) / (L * R)))
-        off += R * L
+        off += (R - 1) * L
         L *= R
     return np.array(tab), [None] + offs
 
@@ -51,7 +51,7 @@ def model_fft(x, E, inv=False):
                 k = b & (L - 1)
                 a = np.array([regs[t][q + B * j] for j in range(R)])
                 if L > 1:
-                    a = a * np.array([1] + [tab[offs[s] + j * L + k] for j in range(1, R)])
+                    a = a * np.array([1] + [tab[offs[s] + (j - 1) * L + k] for j in range(1, R)])
                 y = D @ a
                 for m in range(R):
                     if last:

@@ -54,8 +54,9 @@ Physics physics(double energy, double dz) {
 }
 
 // ----------------------------------------------------------------------------
-// twiddle tables: per Stockham stage s >= 1, W_{L R}^{j k} laid out [j][k],
-// each float64 value stored as float hi + lo parts (re_hi, im_hi, re_lo, im_lo)
+// twiddle tables: per Stockham stage s >= 1, W_{L R}^{j k} for j = 1 .. R-1
+// laid out [j-1][k] (row j = 0 is all ones and is not stored), each float64
+// value stored as float hi + lo parts (re_hi, im_hi, re_lo, im_lo)
 // ----------------------------------------------------------------------------
 std::vector<float4> twiddle_table(int n, int e) {
   const PlanShape p = make_plan_shape(n, e);
@@ -63,13 +64,13 @@ std::vector<float4> twiddle_table(int n, int e) {
   for (int s = 1; s < p.stages; ++s) {
     const int R = p.radix(s), L = p.span(s), off = p.tw_offset(s);
     const long long LR = (long long)L * R;
-    for (int j = 0; j < R; ++j)
+    for (int j = 1; j < R; ++j)
       for (int k = 0; k < L; ++k) {
         const long long m = ((long long)j * k) % LR;
         const double ang = -2.0 * M_PI * (double)m / (double)LR;
         const double c = std::cos(ang), sn = std::sin(ang);
         const float ch = (float)c, sh = (float)sn;
-        tw[off + j * L + k] = make_float4(ch, sh, (float)(c - (double)ch), (float)(sn - (double)sh));
+        tw[off + (j - 1) * L + k] = make_float4(ch, sh, (float)(c - (double)ch), (float)(sn - (double)sh));
       }
   }
   return tw;

@@ -46,10 +46,11 @@ struct FFTPlan {
     for (int i = 0; i < s; ++i) L *= radix(i);
     return L;
   }
-  // offset of stage s in the concatenated twiddle table (stages s >= 1)
+  // offset of stage s in the concatenated twiddle table (stages s >= 1; a
+  // stage holds rows j = 1 .. R-1 of its [j][k] table, row 0 being all ones)
   __host__ __device__ static constexpr int tw_offset(int s) {
     int off = 0;
-    for (int i = 1; i < s; ++i) off += radix(i) * span(i);
+    for (int i = 1; i < s; ++i) off += (radix(i) - 1) * span(i);
     return off;
   }
   static constexpr int TW_SIZE = tw_offset(S) > 0 ? tw_offset(S) : 1;
@@ -66,7 +67,7 @@ struct PlanShape {
   }
   __host__ __device__ int tw_offset(int s) const {
     int off = 0;
-    for (int i = 1; i < s; ++i) off += radix(i) * span(i);
+    for (int i = 1; i < s; ++i) off += (radix(i) - 1) * span(i);
     return off;
   }
   __host__ __device__ int tw_size() const { int t = tw_offset(stages); return t > 0 ? t : 1; }
@@ -309,7 +310,7 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
     if constexpr (L > 1) {
 #pragma unroll
       for (int j = 1; j < R; ++j) {
-        const float4 w = tw[OFF + j * L + k];
+        const float4 w = tw[OFF + (j - 1) * L + k];
         a[j] = INV ? cmulc_tw(a[j], w) : cmul_tw(a[j], w);
       }
     }

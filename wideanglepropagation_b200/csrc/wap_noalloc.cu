@@ -53,8 +53,8 @@ int noalloc_scratch(void** out) {
 }
 }  // namespace
 
-// One thread per table entry: W_{LR}^{jk} of stage s >= 1 at
-// tw_offset(s) + j L + k, float64 value split into float hi + lo.
+// One thread per table entry: W_{LR}^{jk} (j >= 1) of stage s >= 1 at
+// tw_offset(s) + (j - 1) L + k, float64 value split into float hi + lo.
 __global__ void twiddle_fill_kernel(float4* __restrict__ tw, int n, int e) {
   const PlanShape p = make_plan_shape(n, e);
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -68,7 +68,7 @@ __global__ void twiddle_fill_kernel(float4* __restrict__ tw, int n, int e) {
   while (s + 1 < p.stages && idx >= p.tw_offset(s + 1)) ++s;
   const int R = p.radix(s), L = p.span(s);
   const int local = idx - p.tw_offset(s);
-  const int j = local / L, k = local - j * L;
+  const int j = local / L + 1, k = local - (j - 1) * L;
   const long long LR = (long long)L * R;
   const long long m = ((long long)j * k) % LR;
   double sn, c;

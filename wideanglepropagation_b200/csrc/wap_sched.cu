@@ -129,7 +129,7 @@ struct SchedClass {
   float* grad;                  // (draws, N, n, n) probe sums of Re(conj(lambda_a) i a_s)
   float ri_a, ri_inv_den, kphase, e_plus_e0;
   const float4* tw;             // twiddles for (n, E) in global memory
-  int tw_off, tw_len;           // their place in the shared-memory copy
+  int tw_off, tw_len;           // their place in the shared-memory image
   float scale;                  // 1 / (n n)  (also folded into ttab)
   float inv_scale;              // n n
 };
@@ -158,6 +158,8 @@ struct alignas(64) SchedParams {
   int stall_pass;                  // test hook: tiles of this step wait forever (-1: off)
   int checks;                      // validate every task before use (debug)
   int tw_in_smem;                  // twiddles copied to shared memory (else read via L1)
+  const float4* tw_image;          // the shared-memory twiddle image of all classes
+  int tw_image_len;                // its entries
   int stage2;                      // how adjoint rows get psi_s: kPsiGlobal / kPsiStage2 / kPsiSplit
   int* debug;                      // [code, cls, step, b, tile, extra] of the first bad task
 };
@@ -610,10 +612,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   __shared__ Task s_task;
 
   if (P.tw_in_smem) {
-    for (int ci = 0; ci < P.n_classes; ++ci) {
-      const SchedClass& c = P.cls[ci];
-      for (int i = threadIdx.x; i < c.tw_len; i += blockDim.x) tw_smem[c.tw_off + i] = c.tw[i];
-    }
+    for (int i = threadIdx.x; i < P.tw_image_len; i += blockDim.x) tw_smem[i] = P.tw_image[i];
   }
   if (threadIdx.x == 0) {
     mbar_init(&full, 1);
@@ -983,6 +982,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   s->grad = ckpt_every > 0;
   s->ckpt_every = ckpt_every;
   cudaError_t e;
+  int rc0 = WAP_OK;
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
   // elements per thread of the scheduler's transforms (16; 8 for A/B timing)
@@ -992,29 +992,65 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   }
   s->e = E;
   unsigned mask = 0;
-  int tw_total = 0;
   for (int ci = 0; ci < n_classes; ++ci) {
     const int n = classes[ci].n;
     if (!sched_size_ok(n)) return fail(WAP_ERR_UNSUPPORTED, "scan grids must be 128, 256, 512 or 1024 (got %d)", n);
     mask |= n == 128 ? 1u : n == 256 ? 2u : n == 512 ? 4u : 8u;
-    tw_total += make_plan_shape(n, E).tw_size();
   }
+  // Shared-memory twiddle image: the tables of all classes, largest first; a
+  // table equal to the start of one already placed (256 within 512 and 1024:
+  // their first stages are the same radix-16 stage) reuses those entries.
+  std::vector<std::vector<float4>> tables(n_classes);
+  std::vector<int> image_off(n_classes, -1);
+  std::vector<float4> image;
+  {
+    std::vector<int> order(n_classes);
+    for (int ci = 0; ci < n_classes; ++ci) {
+      tables[ci] = twiddle_table(classes[ci].n, E);
+      order[ci] = ci;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return tables[a].size() > tables[b].size(); });
+    for (int ci : order) {
+      const std::vector<float4>& t = tables[ci];
+      for (int cj : order) {
+        if (image_off[cj] < 0 || tables[cj].size() < t.size()) continue;
+        if (!memcmp(tables[cj].data(), t.data(), t.size() * sizeof(float4))) {
+          image_off[ci] = image_off[cj];
+          break;
+        }
+      }
+      if (image_off[ci] < 0) {
+        image_off[ci] = (int)image.size();
+        image.insert(image.end(), t.begin(), t.end());
+      }
+    }
+  }
+  const int tw_total = (int)image.size();
   s->kernel = E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask);
   if (s->grad) s->kernel_bwd = pick_grad(mask);
   // Keep the twiddles in shared memory only when they fit next to the stage
-  // and exchange buffers without lowering the CTAs per SM (3 for E = 16,
-  // 4 for E = 8).
+  // and exchange buffers without lowering the CTAs per SM.
   const size_t base_smem = kTileBytesFor(E) + kExchBytesFor(E);
-  const int want_ctas = E == 16 ? 3 : 4;
-  s->params.tw_in_smem = want_ctas * (base_smem + (size_t)tw_total * sizeof(float4) + 1024) <= 227 * 1024;
+  const size_t tw_smem_bytes = (size_t)tw_total * sizeof(float4);
+  auto ctas_per_sm = [&](ScanKernel k, size_t bytes, int* out) -> int {
+    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaFuncSetAttribute(scan_kernel)");
+    *out = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k, kBlockThreads, bytes);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaOccupancyMaxActiveBlocksPerMultiprocessor(scan_kernel)");
+    return WAP_OK;
+  };
+  int per_sm_tw = 0;
+  if ((rc0 = ctas_per_sm(s->kernel, base_smem, &per_sm)) || (rc0 = ctas_per_sm(s->kernel, base_smem + tw_smem_bytes, &per_sm_tw)))
+    return rc0;
+  s->params.tw_in_smem = per_sm_tw >= per_sm && per_sm_tw > 0;
   if (const char* ov = getenv("WAP_SCHED_TWIDDLES")) {   // debugging / A-B timing only
     if (!strcmp(ov, "smem")) s->params.tw_in_smem = 1;
     if (!strcmp(ov, "global")) s->params.tw_in_smem = 0;
   }
-  s->smem = base_smem + (s->params.tw_in_smem ? (size_t)tw_total * sizeof(float4) : 0);
-  if ((e = cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem)) != cudaSuccess)
-    return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kernel, kBlockThreads, s->smem);
+  s->smem = base_smem + (s->params.tw_in_smem ? tw_smem_bytes : 0);
+  if ((rc0 = ctas_per_sm(s->kernel, s->smem, &per_sm))) return rc0;
   if (per_sm < 1) return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
   s->grid = sms * per_sm;
   if (s->grad) {
@@ -1025,14 +1061,17 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     }
     s->smem_bwd = s->smem + (s->psi_mode == kPsiStage2 ? kTileBytesFor(E) : 0);
     int per_sm_bwd = 0;
-    if ((e = cudaFuncSetAttribute(s->kernel_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem_bwd)) !=
-        cudaSuccess)
-      return cuda_fail(e, "cudaFuncSetAttribute(scan_kernel)");
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_bwd, s->kernel_bwd, kBlockThreads, s->smem_bwd);
+    if ((rc0 = ctas_per_sm(s->kernel_bwd, s->smem_bwd, &per_sm_bwd))) return rc0;
     if (per_sm_bwd < 1) return fail(WAP_ERR_CUDA, "scan_kernel (backward) does not fit on an SM");
     s->grid_bwd = sms * per_sm_bwd;
   }
-  int tw_off = 0;
+  {
+    float4* dimg = nullptr;
+    if ((rc0 = upload(&dimg, image, "twiddle image upload")) != WAP_OK) return rc0;
+    s->d_tw.push_back(dimg);
+    s->params.tw_image = dimg;
+    s->params.tw_image_len = tw_total;
+  }
 
   std::vector<SchedDesc> desc, desc_bwd;
   std::vector<Step> steps_all, steps_bwd_all;
@@ -1076,14 +1115,13 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
       return cuda_fail(e, "cudaMalloc(interleaved H)");
     s->d_hq.push_back(dhq);
     sc.Hq = dhq;
-    std::vector<float4> h = twiddle_table(n, E);
+    const std::vector<float4>& h = tables[ci];
     float4* dtw = nullptr;
     if ((rc = upload(&dtw, h, "twiddle upload")) != WAP_OK) return rc;
     s->d_tw.push_back(dtw);
     sc.tw = dtw;
-    sc.tw_off = tw_off;
+    sc.tw_off = image_off[ci];
     sc.tw_len = (int)h.size();
-    tw_off += sc.tw_len;
     const size_t tt = (size_t)c.n_draws * c.n_slices * n * n;
     float2* dtt = nullptr;
     if ((e = cudaMalloc(&dtt, tt * sizeof(float2))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(transmission table)");
