@@ -55,6 +55,14 @@ int wap_plan_destroy(wap_plan* plan);
 int wap_plan_set_config(wap_plan* plan, int row_e, int col_e, int col_w);
 int wap_plan_get_config(const wap_plan* plan, int* row_e, int* col_e, int* col_w);
 
+/* Detector window of the diffraction pattern for the plan's later calls:
+ * the last column pass stores only rows y0 .. y0+ny-1 and columns
+ * x0 .. x0+nx-1 of the fftshifted |fft2(exit)|^2, so dp (and grad_dp of
+ * wap_multislice_bwd) is (n_probes, ny, nx).  The centre crop of
+ * downsample_to_max_angle / max_angle_gpts (propagation.py:394-439) fused
+ * into the diffraction epilogue.  ny = nx = 0: the whole grid (default). */
+int wap_plan_set_detector(wap_plan* plan, int y0, int x0, int ny, int nx);
+
 /* Transfer function on the device, evaluated in float64.
  *   WAP_TF_FRESNEL: propagation.py:139-145
  *       H[i,j] = exp(i 2 pi z/lam) exp(-i pi lam z (fx_i^2 + fy_j^2))
@@ -156,8 +164,10 @@ typedef struct wap_scan_class {
   const float* H_lo;         /* (n, n) complex64 remainder or NULL */
   double dz, energy;
   float* exit;               /* (n_probes, n, n) complex64: working buffer, exit waves */
-  float* dp;                 /* (n_probes, n, n) float32 or NULL */
+  float* dp;                 /* (n_probes, n, n) float32, or (n_probes, det_ny, det_nx), or NULL */
   int group;                 /* probes advanced together (0: automatic) */
+  int det_y0, det_x0;        /* detector window of dp (see wap_plan_set_detector); */
+  int det_ny, det_nx;        /*   det_ny = det_nx = 0: the whole grid */
 } wap_scan_class;
 
 typedef struct wap_scan wap_scan;

@@ -63,6 +63,25 @@ def test_detector_crop_matches_oracle(golden):
                           golden["crop_even"])
 
 
+@pytest.mark.parametrize("shape,sampling,energy,angle,parity", [
+    ((64, 64), (0.1, 0.1), 200e3, 40.0, "odd"),
+    ((128, 64), (0.05, 0.08), 300e3, 25.0, "even"),
+    ((256, 256), (0.05, 0.05), 300e3, 60.0, "odd"),
+    ((32, 32), (0.2, 0.2), 80e3, 1e5, "odd"),
+])
+def test_detector_window_is_the_oracle_crop(shape, sampling, energy, angle, parity):
+    """The fused crop's window selects the same pixels as the oracle's
+    downsample_to_max_angle (propagation.py:424-439) of the full pattern."""
+    idx = np.arange(shape[0] * shape[1]).reshape(shape)
+    ref = O.downsample_to_max_angle(idx, sampling, O.energy2wavelength(energy), angle, parity=parity)
+    win = wap.detector_window(shape, sampling, energy, angle, parity)
+    if win is None:
+        assert ref.shape == shape
+        return
+    y0, x0, ny, nx = win
+    assert np.array_equal(idx[y0:y0 + ny, x0:x0 + nx], ref)
+
+
 def test_move_probe_matches_golden(golden):
     for pos, want in zip(golden["mp_pos"], golden["mp_out"]):
         assert np.array_equal(wap.move_probe(golden["mp_in"], tuple(pos)).numpy(), want)

@@ -35,6 +35,7 @@ SIGNATURES = {
     "wap_plan_create": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I, _I]),
     "wap_plan_destroy": (_I, [_P]),
     "wap_plan_set_config": (_I, [_P, _I, _I, _I]),
+    "wap_plan_set_detector": (_I, [_P, _I, _I, _I, _I]),
     "wap_plan_get_config": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_transfer_function": (_I, [_I, _I, _I, _D, _D, _D, _D, _P, _I, _P, _P]),
     "wap_multislice_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
@@ -67,7 +68,8 @@ class ScanClass(ctypes.Structure):
     """Mirror of ``wap_scan_class`` (include/wap.h)."""
     _fields_ = [("n", _I), ("n_slices", _I), ("n_draws", _I), ("n_probes", _I),
                 ("V", _P), ("draw", _P), ("psi0", _P), ("positions", _P), ("H", _P), ("H_lo", _P),
-                ("dz", _D), ("energy", _D), ("exit", _P), ("dp", _P), ("group", _I)]
+                ("dz", _D), ("energy", _D), ("exit", _P), ("dp", _P), ("group", _I),
+                ("det_y0", _I), ("det_x0", _I), ("det_ny", _I), ("det_nx", _I)]
 
 
 _lib = None

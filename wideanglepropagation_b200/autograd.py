@@ -24,20 +24,13 @@ import ctypes
 import threading
 
 from . import _lib
-from .propagation import SCAN_MIN_PROBES, SCAN_SIZES, _device, _prepare, _ptr, _stream, get_plan, split_transfer
+from .propagation import (SCAN_MIN_PROBES, SCAN_SIZES, _detector, _device, _dp_shape, _prepare, _ptr, _stream,
+                          get_plan, scan_class, split_transfer)
 
 # gradient scans (persistent scheduler) by shape; a scan is held from the
 # forward until its backward has run, so several pending graphs get their own
 _pool: dict = {}
 _pool_lock = threading.Lock()
-
-
-def _scan_class(V, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp):
-    D, N, n, _ = V.shape
-    return _lib.ScanClass(n, N, D, exit_wave.shape[0], V.data_ptr(), dr.data_ptr() if dr is not None else None,
-                          psi.data_ptr(), pos.data_ptr() if pos is not None else None, Hc.data_ptr(),
-                          Hl.data_ptr() if Hl is not None else None, float(dz), float(energy), exit_wave.data_ptr(),
-                          dp.data_ptr(), 0)
 
 
 def _acquire(key, cls, k):
@@ -62,7 +55,7 @@ def _release(key, h):
 
 class MultisliceFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every):
+    def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every, det):
         dev = V.device
         ctx.set_materialize_grads(False)
         Vc, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(V.detach(), probe, positions, draw, dev)
@@ -71,24 +64,25 @@ class MultisliceFunction(torch.autograd.Function):
         if ctx.needs_input_grad[0] and ny == nx and ny in SCAN_SIZES and B >= SCAN_MIN_PROBES and not per_probe:
             # persistent scheduler: forward with checkpoints now, adjoint later
             exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-            dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+            dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
             k = max(1, min(int(ckpt_every), N))
             key = (torch.cuda.current_device(), ny, N, Vc.shape[0], B, k)
-            h = _acquire(key, _scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp), k)
+            h = _acquire(key, scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp, det), k)
             _lib.check(_lib.lib().wap_scan_run(h, _stream()))
             ctx.scan = (key, h)
             # everything the scan reads in the backward must outlive it
             ctx.keep = (Vc, psi, pos, dr, Hc, Hl, exit_wave, dp)
             ctx.save_for_backward(Vc)
-            ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched)
+            ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched, det)
             if not batched:
                 return exit_wave[0], dp[0]
             return exit_wave, dp
         plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
+        plan.set_detector(det)
         k = max(1, int(ckpt_every))
         nck = (N + k - 1) // k
         exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-        dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+        dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
         ckpt = torch.empty((B, nck, ny, nx), dtype=torch.complex64, device=dev)
         _lib.check(_lib.lib().wap_multislice_fwd_ckpt(
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
@@ -97,7 +91,7 @@ class MultisliceFunction(torch.autograd.Function):
         empty = torch.empty(0, device=dev)
         ctx.save_for_backward(Vc, Hc, Hl if Hl is not None else empty, exit_wave, ckpt,
                               dr if dr is not None else empty)
-        ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched)
+        ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched, det)
         if not batched:
             return exit_wave[0], dp[0]
         return exit_wave, dp
@@ -107,42 +101,45 @@ class MultisliceFunction(torch.autograd.Function):
         if ctx.scan is not None:
             key, h = ctx.scan
             (Vc,) = ctx.saved_tensors
-            B, N, ny, nx, dz, energy, k, has_draw, vshape, batched = ctx.meta
+            B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta
             try:
                 if g_exit is None and g_dp is not None:
                     grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=Vc.device)
-                    g = g_dp.to(torch.float32).reshape(B, ny, nx).contiguous()
+                    g = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
                     _lib.check(_lib.lib().wap_scan_grad_backward(h, _ptr(g), _ptr(grad_V), _stream()))
-                    return grad_V.reshape(vshape), None, None, None, None, None, None, None
+                    return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
             finally:
                 _release(key, h)
             # a loss on the exit wave: the per-pass adjoint below needs its own checkpoints
             Vc2, psi, pos, dr, Hc, Hl, _, _ = ctx.keep
-            return _per_pass_backward(Vc2, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp)
+            return _per_pass_backward(Vc2, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp,
+                                      det)
         Vc, Hc, Hl, exit_wave, ckpt, dr = ctx.saved_tensors
-        B, N, ny, nx, dz, energy, k, has_draw, vshape, batched = ctx.meta
+        B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta
         dev = Vc.device
         plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
+        plan.set_detector(det)
         if g_exit is not None:
             g_exit = g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
         if g_dp is not None:
-            g_dp = g_dp.to(torch.float32).reshape(B, ny, nx).contiguous()
+            g_dp = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
         grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=dev)
         work = torch.empty((B, k + 2, ny, nx), dtype=torch.complex64, device=dev)
         _lib.check(_lib.lib().wap_multislice_bwd(
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr) if has_draw else None, B, _ptr(Hc),
             _ptr(Hl) if Hl.numel() else None, dz, energy,
             _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
-        return grad_V.reshape(vshape), None, None, None, None, None, None, None
+        return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
 
 
-def _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp):
+def _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp, det):
     """Checkpointed forward + hand-written adjoint with the per-pass kernels."""
     dev = Vc.device
     plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
+    plan.set_detector(det)
     nck = (N + k - 1) // k
     exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-    dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+    dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
     ckpt = torch.empty((B, nck, ny, nx), dtype=torch.complex64, device=dev)
     _lib.check(_lib.lib().wap_multislice_fwd_ckpt(
         plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), _ptr(psi), B, 0, _ptr(pos), _ptr(Hc), _ptr(Hl),
@@ -150,20 +147,23 @@ def _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vs
     if g_exit is not None:
         g_exit = g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
     if g_dp is not None:
-        g_dp = g_dp.to(torch.float32).reshape(B, ny, nx).contiguous()
+        g_dp = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
     grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=dev)
     work = torch.empty((B, k + 2, ny, nx), dtype=torch.complex64, device=dev)
     _lib.check(_lib.lib().wap_multislice_bwd(
         plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), B, _ptr(Hc), _ptr(Hl), dz, energy,
         _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
-    return grad_V.reshape(vshape), None, None, None, None, None, None, None
+    return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
 
 
 def simulate_fresnel_as_differentiable(potential: torch.Tensor, probe, prop_kernel, slice_thickness, energy, *,
-                                       positions=None, draw=None, ckpt_every: int | None = None):
+                                       positions=None, draw=None, ckpt_every: int | None = None,
+                                       max_angle=None, sampling=None, parity="odd"):
     """(exit_wave, diffraction_pattern) with gradients flowing to ``potential``.
 
     ``ckpt_every`` defaults to round(sqrt(N)) slices between saved waves.
+    ``max_angle`` / ``sampling`` / ``parity``: the pattern is cropped to the
+    detector window as in ``simulate_fresnel_as`` (the loss sees only it).
     """
     _device()
     if not isinstance(potential, torch.Tensor):
@@ -171,5 +171,6 @@ def simulate_fresnel_as_differentiable(potential: torch.Tensor, probe, prop_kern
     N = potential.shape[-3]
     if ckpt_every is None:
         ckpt_every = max(1, int(round(math.sqrt(N))))
+    det = _detector(tuple(potential.shape[-2:]), sampling, energy, max_angle, parity)
     return MultisliceFunction.apply(potential, probe, prop_kernel, slice_thickness, energy, positions, draw,
-                                    ckpt_every)
+                                    ckpt_every, det)

@@ -335,6 +335,20 @@ int wap_plan_set_config(wap_plan* p, int row_e, int col_e, int col_w) {
   return upload_twiddles(p);
 }
 
+int wap_plan_set_detector(wap_plan* p, int y0, int x0, int ny, int nx) {
+  clear_error();
+  if (!p) return fail(WAP_ERR_ARG, "plan is NULL");
+  if (ny == 0 && nx == 0) {
+    p->det = Detector{};
+    return WAP_OK;
+  }
+  if (ny < 1 || nx < 1 || y0 < 0 || x0 < 0 || y0 + ny > p->ny || x0 + nx > p->nx)
+    return fail(WAP_ERR_ARG, "detector window rows %d+%d, columns %d+%d outside the %d x %d grid", y0, ny, x0, nx,
+                p->ny, p->nx);
+  p->det = Detector{y0, x0, ny, nx};
+  return WAP_OK;
+}
+
 int wap_plan_get_config(const wap_plan* p, int* row_e, int* col_e, int* col_w) {
   clear_error();
   if (!p || !row_e || !col_e || !col_w) return fail(WAP_ERR_ARG, "NULL argument");
@@ -407,6 +421,7 @@ ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo) {
   c.ny = p->ny;
   c.nx = p->nx;
   c.seed_scale = (float)((double)p->ny * p->nx);
+  c.det = p->det;
   return c;
 }
 

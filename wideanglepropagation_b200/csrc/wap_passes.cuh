@@ -84,8 +84,9 @@ struct ColArgs {
   const float2* H;           // (ny, nx)
   const float2* H_lo;        // (ny, nx) H - H rounded to complex64, or null
   const float4* tw;          // twiddle table for ny (hi, lo)
-  float* dp;                 // COL_DP: (B, ny, nx)
-  const float* g;            // COL_SEED: dL/ddp (B, ny, nx), fftshifted like dp
+  float* dp;                 // COL_DP: (B, det window) or (B, ny, nx)
+  const float* g;            // COL_SEED: dL/ddp laid out like dp (zero outside the window)
+  Detector det;              // diffraction-pattern window of dp / g
   const float2* seed2;       // COL_SEED: optional row-transformed lambda_exit
   long long seed2_bstride;
   int ny, nx;
@@ -331,12 +332,13 @@ col_pass_kernel(const ColArgs a) {
   // fftshift of (ky, kx) for dp / g
   const int sx = (col + (nx >> 1)) & (nx - 1);
   if constexpr (SEED) {
-    const float* gp = a.g + (long long)b * plane;
+    const float* gp = a.g + (long long)b * a.det.plane(NY, nx);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int ky = t + T * e;
       const int sy = (ky + (NY >> 1)) & (NY - 1);
-      v[e] = a.g ? cscale(v[e], a.seed_scale * __ldg(gp + (long long)sy * nx + sx)) : make_float2(0.f, 0.f);
+      const long long gi = a.det.index(sy, sx, nx);
+      v[e] = (a.g && gi >= 0) ? cscale(v[e], a.seed_scale * __ldg(gp + gi)) : make_float2(0.f, 0.f);
     }
     if (a.seed2) {
       float2 u[E];
@@ -378,12 +380,13 @@ col_pass_kernel(const ColArgs a) {
   }
 
   if (f & COL_DP) {
-    float* dp = a.dp + (long long)b * plane;
+    float* dp = a.dp + (long long)b * a.det.plane(NY, nx);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int ky = t + T * e;
       const int sy = (ky + (NY >> 1)) & (NY - 1);
-      __stcs(dp + (long long)sy * nx + sx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      const long long di = a.det.index(sy, sx, nx);
+      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
     if (f & COL_NO_H) return;  // pure diffraction epilogue: no inverse transform
   }
@@ -478,7 +481,8 @@ struct WpmColArgs {
   const float* refs;         // (draws, n_slices, K)
   const int* draw;
   const float4* tw;
-  float* dp;                 // dp mode: |fft2|^2 (fftshifted), no fields
+  float* dp;                 // dp mode: |fft2|^2 (fftshifted, detector window), no fields
+  Detector det;
   int ny, nx, K, slice, n_slices, probe0, dp_mode;
   float k02;                 // k0^2
   float dz;
@@ -517,12 +521,13 @@ wpm_col_kernel(const WpmColArgs a) {
   fft<NY, E, false>(v, t, xs, tw);
 
   if (a.dp_mode) {
-    float* dp = a.dp + (long long)b * plane;
+    float* dp = a.dp + (long long)b * a.det.plane(NY, nx);
     const int sx = (col + (nx >> 1)) & (nx - 1);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int sy = (t + T * e + (NY >> 1)) & (NY - 1);
-      __stcs(dp + (long long)sy * nx + sx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      const long long di = a.det.index(sy, sx, nx);
+      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
     return;
   }

@@ -116,7 +116,8 @@ struct SchedClass {
   const float2* ttab;           // (draws, N, n, n)  t / (n n)
   long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
-  float* dp;                    // (B, n, n) or null
+  float* dp;                    // (B, n, n), (B, detector window) or null
+  Detector det;                 // window of dp and g
   // gradient buffers
   float2* lam;                  // (B, n, n) adjoint state
   float2* work;                 // (B, n, n) recompute buffer
@@ -481,11 +482,13 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
   if constexpr (GRAD) {
     if (type == ST_SEED_COL) {
       // lambda seed: n^2 g Z with g = dL/d(dp) at the fftshifted position
-      const float* gp = c.g + (long long)k.b * plane;
+      // (zero outside the detector window)
+      const float* gp = c.g + (long long)k.b * c.det.plane(N, N);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int sy = (t + T * e + (N >> 1)) & (N - 1);
-        v[e] = cscale(v[e], c.inv_scale * __ldg(gp + (long long)sy * N + sx));
+        const long long gi = c.det.index(sy, sx, N);
+        v[e] = gi >= 0 ? cscale(v[e], c.inv_scale * __ldg(gp + gi)) : make_float2(0.f, 0.f);
       }
     }
   }
@@ -505,11 +508,12 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     }
   }
   if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
-    float* dp = c.dp + (long long)k.b * plane;
+    float* dp = c.dp + (long long)k.b * c.det.plane(N, N);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int sy = (t + T * e + (N >> 1)) & (N - 1);
-      __stcs(dp + (long long)sy * N + sx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      const long long di = c.det.index(sy, sx, N);
+      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
   }
   fft<N, E, true>(v, t, xs, tw);
@@ -866,6 +870,20 @@ static void scan_free(wap_scan* s) {
 
 static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n == 1024; }
 
+// detector window of a class's diffraction patterns (0 x 0: the whole grid)
+static int class_detector(const wap_scan_class& c, int ci, Detector* d) {
+  if (c.det_ny == 0 && c.det_nx == 0) {
+    *d = Detector{};
+    return WAP_OK;
+  }
+  if (c.det_ny < 1 || c.det_nx < 1 || c.det_y0 < 0 || c.det_x0 < 0 || c.det_y0 + c.det_ny > c.n ||
+      c.det_x0 + c.det_nx > c.n)
+    return fail(WAP_ERR_ARG, "scan class %d: detector window rows %d+%d, columns %d+%d outside the %d x %d grid", ci,
+                c.det_y0, c.det_ny, c.det_x0, c.det_nx, c.n, c.n);
+  *d = Detector{c.det_y0, c.det_x0, c.det_ny, c.det_nx};
+  return WAP_OK;
+}
+
 // column-tile tensor map over (B n rows) x (n columns) of 8-byte elements
 static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map, void* base, int n, int n_probes,
                       int cols_w, int box_rows) {
@@ -1101,6 +1119,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     sc.draw = c.draw;
     sc.V = c.V;
     sc.dp = c.dp;
+    if ((rc0 = class_detector(c, ci, &sc.det))) return rc0;
     sc.vstride = (long long)c.n_slices * n * n;
     sc.scale = (float)(1.0 / ((double)n * n));
     sc.inv_scale = (float)((double)n * n);
@@ -1334,6 +1353,7 @@ int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
     sc.draw = c.draw;
     sc.V = c.V;
     sc.dp = c.dp;
+    if ((rc = class_detector(c, ci, &sc.det))) return rc;
     s->cls[ci] = c;
     s->phys[ci] = physics(c.energy, c.dz);
     const Physics& ph = s->phys[ci];

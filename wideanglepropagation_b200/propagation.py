@@ -17,6 +17,10 @@ reference behaviour):
   scan is one call.
 * a (B, ny, nx) probe runs B independent probes; a (D, N, ny, nx) potential
   holds D frozen-phonon draws selected per probe by ``draw``.
+* ``max_angle`` (mrad) with ``sampling`` and ``parity`` - the diffraction
+  pattern comes back already cropped to the detector window that
+  ``downsample_to_max_angle`` (propagation.py:424-439) would keep; the crop is
+  fused into the last column pass, which stores only that window.
 """
 from __future__ import annotations
 
@@ -41,7 +45,7 @@ __all__ = [
     "angular_spectrum_propagation_kernel", "Propagator", "wpm_step_adaptive",
     "move_probe", "transmission_function", "simulate_fresnel_as",
     "simulate_fresnel_as_jit", "simulate_fresnel", "simulate_wpm",
-    "simulate_wpm_jit", "max_angle_gpts", "downsample_to_max_angle",
+    "simulate_wpm_jit", "max_angle_gpts", "downsample_to_max_angle", "detector_window",
 ]
 
 
@@ -106,9 +110,17 @@ class Plan:
         self.handle = h
         self.ny, self.nx, self.max_batch, self.op, self.n_bins = ny, nx, max_batch, op, n_bins
         self.device = torch.cuda.current_device()
+        self.det = None
 
     def set_config(self, row_e: int, col_e: int, col_w: int) -> None:
         _lib.check(_lib.lib().wap_plan_set_config(self.handle, row_e, col_e, col_w))
+
+    def set_detector(self, det) -> None:
+        """Diffraction-pattern window (y0, x0, ny, nx) of later calls; None: whole grid."""
+        if det != self.det:
+            y0, x0, dny, dnx = det if det is not None else (0, 0, 0, 0)
+            _lib.check(_lib.lib().wap_plan_set_detector(self.handle, y0, x0, dny, dnx))
+            self.det = det
 
     def config(self) -> tuple:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -151,6 +163,7 @@ def get_plan(ny: int, nx: int, batch: int, op: int, n_bins: int = 0) -> Plan:
             if cfg is not None:
                 p.set_config(*cfg)
             _plans[key] = p
+        p.set_detector(None)   # cached plans are shared: whole-grid patterns unless a caller sets a window
         return p
 
 
@@ -299,17 +312,47 @@ _scans: dict = {}
 _scans_lock = threading.Lock()
 
 
-def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp):
+def detector_window(shape, sampling, energy, max_angle, parity="odd"):
+    """(y0, x0, ny, nx) of the centre crop ``downsample_to_max_angle`` keeps of
+    an fftshifted pattern (propagation.py:424-439), or None for the whole grid."""
+    ny, nx = shape
+    dny, dnx = max_angle_gpts((ny, nx), sampling, energy2wavelength(float(energy)), max_angle, parity=parity)
+    if (dny, dnx) == (ny, nx):
+        return None
+    return ny // 2 - dny // 2, nx // 2 - dnx // 2, dny, dnx
+
+
+def _detector(shape, sampling, energy, max_angle, parity):
+    if max_angle is None:
+        return None
+    if sampling is None:
+        raise ValueError("max_angle needs the grid sampling")
+    return detector_window(shape, _pair(sampling), energy, max_angle, parity)
+
+
+def _dp_shape(B, ny, nx, det):
+    return (B, det[2], det[3]) if det is not None else (B, ny, nx)
+
+
+def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, group=0):
+    """``wap_scan_class`` for one grid class of device tensors."""
+    D, N, n, _ = V.shape
+    y0, x0, dny, dnx = det if det is not None else (0, 0, 0, 0)
+    return _lib.ScanClass(n, N, D, exit_wave.shape[0], V.data_ptr(), dr.data_ptr() if dr is not None else None,
+                          psi.data_ptr(), pos.data_ptr() if pos is not None else None, H.data_ptr(),
+                          H_lo.data_ptr() if H_lo is not None else None, float(dz), float(energy),
+                          exit_wave.data_ptr(), dp.data_ptr() if dp is not None else None, int(group),
+                          y0, x0, dny, dnx)
+
+
+def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None):
     """Run a batched forward through the persistent scheduler (cached per shape)."""
     D, N, n, _ = V.shape
     B = exit_wave.shape[0]
     dev = torch.cuda.current_device()
     key = (dev, n, N, D, B)
     cls = (_lib.ScanClass * 1)()
-    cls[0] = _lib.ScanClass(n, N, D, B, V.data_ptr(), dr.data_ptr() if dr is not None else None, psi.data_ptr(),
-                            pos.data_ptr() if pos is not None else None, H.data_ptr(),
-                            H_lo.data_ptr() if H_lo is not None else None, float(dz), float(energy),
-                            exit_wave.data_ptr(), dp.data_ptr(), 0)
+    cls[0] = scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det)
     L = _lib.lib()
     arr = ctypes.cast(cls, ctypes.c_void_p)
     with _scans_lock:
@@ -324,13 +367,16 @@ def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp):
 
 
 def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, *,
-                        return_wavefronts: bool = True, positions=None, draw=None):
+                        return_wavefronts: bool = True, positions=None, draw=None,
+                        max_angle=None, sampling=None, parity="odd"):
     """Fresnel / angular-spectrum multislice (propagation.py:305-352).
 
     Returns ``(exit_wave, diffraction_pattern, wavefronts)`` where
     ``diffraction_pattern = |fftshift(fft2(exit_wave))|^2`` and
     ``wavefronts`` stacks the wave after every slice (``None`` when
-    ``return_wavefronts=False``).
+    ``return_wavefronts=False``).  With ``max_angle`` (mrad) and ``sampling``
+    the pattern is ``downsample_to_max_angle(pattern, sampling,
+    wavelength, max_angle, parity)``, stored cropped by the kernel.
     """
     dev = _device()
     V, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(potential, probe, positions, draw, dev)
@@ -339,16 +385,18 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     H, H_lo = split_transfer(prop_kernel, dev)
     if H.shape != (ny, nx):
         raise ValueError(f"prop_kernel shape {tuple(H.shape)} does not match grid {(ny, nx)}")
+    det = _detector((ny, nx), sampling, energy, max_angle, parity)
     exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-    dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+    dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
     if (not return_wavefronts and ny == nx and ny in SCAN_SIZES and B >= SCAN_MIN_PROBES
             and not per_probe):
         # many probes of one shared probe: the persistent batched scheduler
-        _scan_run(V, psi, pos, dr, H, H_lo, slice_thickness, energy, exit_wave, dp)
+        _scan_run(V, psi, pos, dr, H, H_lo, slice_thickness, energy, exit_wave, dp, det)
         if not batched:
             exit_wave, dp = exit_wave[0], dp[0]
         return exit_wave, dp, None
     plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
+    plan.set_detector(det)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
@@ -366,13 +414,14 @@ simulate_fresnel = simulate_fresnel_as
 
 
 def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128, power_spacing=2.0, *,
-                 return_wavefronts: bool = True, positions=None, draw=None):
+                 return_wavefronts: bool = True, positions=None, draw=None, max_angle=None, parity="odd"):
     """WPM adaptive-binning multislice (propagation.py:358-387).
 
     Per slice: n_bins reference refractive indices spaced
     n_min + (n_max - n_min) t^power_spacing, one angular-spectrum propagate
     per reference, smoothstep blend of the two bracketing fields per pixel
-    (propagation.py:215-256).  ``sampling`` = (dy, dx).
+    (propagation.py:215-256).  ``sampling`` = (dy, dx).  ``max_angle`` (mrad):
+    the pattern comes back cropped as by ``downsample_to_max_angle``.
     """
     dev = _device()
     V, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(potential, probe, positions, draw, dev)
@@ -383,8 +432,10 @@ def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128
         raise ValueError("n_bins must be >= 2")
     dy, dx = _pair(sampling)
     plan = get_plan(ny, nx, B, _lib.WAP_OP_WPM, n_bins)
+    det = _detector((ny, nx), sampling, energy, max_angle, parity)
+    plan.set_detector(det)
     exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-    dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+    dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
     _lib.check(_lib.lib().wap_wpm_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
