@@ -268,12 +268,7 @@ def main():
     _lib.profile_reset()
     dom = max(kinds, key=lambda k: kinds[k][1])
     n, kms, by = kinds[dom]
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peak = float(json.load(open(peaks_path))["hbm_gbs"])
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = _peak_hbm()
     achieved = by / (kms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": _ncu_traffic(dom), "kernel": dom, "peak_source": peak_src,
@@ -290,9 +285,13 @@ def main():
         extras.update(_configs())
         extras.update(_grad_ratio(args))
         extras.update(_err_vs_fp64(classes, classes_host))
+        extras.update(_lines())
 
     # --- e2e through the public API from pinned host buffers ------------------
     e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
+    if not args.no_extras:
+        # the same with a 50 mrad detector: the crop is fused into the last column pass
+        extras["e2e_detector_50mrad"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=50.0)
 
     cpu = None
     if rank == 0 and not args.no_extras:
@@ -472,6 +471,54 @@ def _grad_ratio(args):
             "grad_workload": "512^2, 64 slices x 2 A, 300 keV, 64 probes (8x8), L = sum(|FFT psi|^2 - I)^2"}
 
 
+def _peak_hbm():
+    """Measured HBM copy bandwidth (GB/s) and its source; the pool's earlier
+    measurement when the measured-peaks file is absent."""
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _lines():
+    """1D helpers: propagate_1d over 65536 lines of 2048 points (1 GiB in,
+    1 GiB out: HBM-bound, 16 B per point) and the naive per-pixel WPM step on
+    64^2 (direct float64 sums)."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    n, L = 2048, 65536
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(0)
+    psi = torch.randn((L, n), dtype=torch.complex64, device=dev, generator=g)
+    kx = wap.get_kx_1d(n, 0.2)
+    H = wap.angular_spectrum_kernel_1d(kx ** 2, 20.0, 3.0)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        wap.propagate_1d(psi, H)
+    torch.cuda.synchronize()
+    reps = 10
+    s.record()
+    for _ in range(reps):
+        wap.propagate_1d(psi, H)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    gbs = 16.0 * n * L / (ms / 1e3) / 1e9
+    peak, peak_src = _peak_hbm()
+    rng = np.random.default_rng(0)
+    wave = rng.normal(size=(64, 64)) + 1j * rng.normal(size=(64, 64))
+    nmap = 1.0 + 1e-4 * rng.random((64, 64))
+    wap.wpm_step(wave, nmap, 2.0, 300e3, (0.05, 0.05))
+    torch.cuda.synchronize()
+    s.record()
+    wap.wpm_step(wave, nmap, 2.0, 300e3, (0.05, 0.05))
+    e.record()
+    torch.cuda.synchronize()
+    return {"lines_1d": {"propagate_1d_ms": ms, "lines": L, "n": n, "achieved_gbs": gbs, "peak_gbs": peak,
+                         "peak_source": peak_src, "frac": gbs / peak, "bytes_per_point": 16},
+            "wpm_naive_step_64x64_ms": s.elapsed_time(e)}
+
+
 def _err_vs_fp64(classes, classes_host):
     import torch
     import wideanglepropagation_b200 as wap
@@ -489,22 +536,28 @@ def _err_vs_fp64(classes, classes_host):
     return {"err_vs_fp64": errs}
 
 
-def _e2e(classes_host, args, dev, barrier, max_over_ranks, world):
+def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None):
+    """The headline workload through simulate_fresnel_as from pinned host
+    buffers; with ``max_angle`` (mrad) the patterns come back cropped to that
+    detector window (the crop fused into the last column pass)."""
     import torch
     import wideanglepropagation_b200 as wap
     host = []
     for w in classes_host:
         V = torch.from_numpy(w.potential).pin_memory()
         H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+        win = wap.detector_window((w.ny, w.nx), (w.ps, w.ps), w.energy, max_angle) if max_angle else None
+        shape = (w.n_probes, win[2], win[3]) if win else (w.n_probes, w.ny, w.nx)
         host.append((w, V, torch.from_numpy(w.probe).pin_memory(), torch.from_numpy(w.positions).pin_memory(),
                      torch.from_numpy(w.draw_of_probe).pin_memory(), H,
-                     torch.empty((w.n_probes, w.ny, w.nx), dtype=torch.float32).pin_memory()))
+                     torch.empty(shape, dtype=torch.float32).pin_memory()))
     h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
     d2h = sum(o.numel() * 4 for *_, o in host)
 
     def step():
         for w, V, p, q, d, H, out in host:
-            _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False)
+            _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False,
+                                               max_angle=max_angle, sampling=(w.ps, w.ps))
             out.copy_(dp, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
@@ -519,8 +572,10 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world):
     torch.cuda.synchronize()
     ms = max_over_ranks(s.elapsed_time(e)) / args.steps
     total = sum(w.n_probes * w.n_slices for w in classes_host)
+    api = "simulate_fresnel_as(positions=, draw=)" if not max_angle else \
+        f"simulate_fresnel_as(positions=, draw=, max_angle={max_angle:g}, sampling=)"
     return {"value": total * world / (ms / 1e3), "unit": "slice-steps/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "simulate_fresnel_as(positions=, draw=)"}
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": api}
 
 
 if __name__ == "__main__":

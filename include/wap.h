@@ -98,6 +98,34 @@ int wap_multislice_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws
                        const float* H_lo, double dz, double energy, float* exit, float* dp,
                        float* stack, void* stream);
 
+/* 1D helpers (propagation.py:609-652) and the naive per-pixel WPM step.
+ *
+ * wap_line_transfer: out (n) complex128 =
+ *   WAP_TF_FRESNEL  exp(-i kx_sq dy / (2 k0))            fresnel_kernel_1d (:617-619)
+ *   WAP_TF_ANGULAR  exp(i dy sqrt(k0^2 - kx_sq)), the principal complex root
+ *                                                        angular_spectrum_kernel_1d (:622-626)
+ *   evaluated in float64; kx_sq is (n) float64.
+ * wap_line_propagate: out[l] = ifft(fft(psi[l]) H) for n_lines complex64 lines of
+ *   n points (a power of two in [32, 2048]): propagate_1d (:629-633).  H is
+ *   (n) complex64 shared by every line, or (n_lines, n) with h_per_line; H_lo
+ *   its float64 remainder or NULL.
+ * wap_line_wpm: out[k] = ifft(psi_k exp(i dy sqrt((n_vals[k] k0)^2 - kx_sq)))
+ *   for n_refs indices: wpm_kernel_1d / wpm_kernel_1d_vmap (:636-652); psi_k is
+ *   one (n) complex64 spectral line, the transfer function is evaluated in
+ *   float64 and applied as hi + lo parts.
+ * wap_wpm_naive_step: wpm_step (:184-212): out[p] = pixel p of
+ *   ifft2(fft2(wave) exp(i dz sqrt((n_map[p] k0)^2 - k_perp^2))) with k_perp
+ *   from get_frequencies(ny, nx, (ps0, ps1)), evaluated as direct float64 sums
+ *   (any ny x nx up to 65536 pixels; O(P^2) work).  wave and out are (ny, nx)
+ *   complex128, n_map (ny, nx) float64, work 2 ny nx complex128. */
+int wap_line_transfer(int kind, int n, const double* kx_sq, double k0, double dy, double* out, void* stream);
+int wap_line_propagate(int n, int n_lines, const float* psi, const float* H, const float* H_lo, int h_per_line,
+                       float* out, void* stream);
+int wap_line_wpm(int n, int n_refs, const float* psi_k, const double* n_vals, double k0, const double* kx_sq,
+                 double dy, float* out, void* stream);
+int wap_wpm_naive_step(int ny, int nx, const double* wave, const double* n_map, double dz, double energy,
+                       double ps0, double ps1, double* out, double* work, void* stream);
+
 /* WPM adaptive-binning multislice forward, propagation.py:358-387 with the
  * step of propagation.py:215-256 (n_bins reference indices spaced
  * n_min + (n_max - n_min) t^power_spacing per slice, smoothstep blend of the

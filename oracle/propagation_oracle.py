@@ -11,12 +11,14 @@ What it restates (reference file ``wide_angle_propagation/propagation.py``):
 * Fresnel and angular-spectrum transfer funcs .. :139-156
 * WPM single-index propagator (+vmap) .......... :159-171
 * ``Propagator`` (fft2 . H . ifft2) .............. :178-181
+* naive ``wpm_step`` (one propagate per pixel) .. :184-212
 * ``wpm_step_adaptive`` .......................... :215-256
 * ``move_probe`` ................................. :263-276
 * ``simulate_fresnel_as`` ........................ :305-352
 * ``simulate_wpm`` ............................... :358-387
 * detector crop ``max_angle_gpts`` /
   ``downsample_to_max_angle`` .................... :394-439
+* 1D helpers ``get_kx_1d`` .. ``wpm_kernel_1d_vmap`` :609-652
 
 Parity pin: the reference module cannot be imported with its real
 dependencies here (jax, jaxlib, abtem and ase are not installed).  The
@@ -198,6 +200,27 @@ def wpm_propagation_kernel(Ek, n_val, k0, k_perp2, dz):
 def Propagator(u, H):
     """ifft2(H * fft2(u)) (propagation.py:178-181)."""
     return _ifft2(H * _fft2(u))
+
+
+# ---------------------------------------------------------------------------
+# propagation.py:184-212
+# ---------------------------------------------------------------------------
+def wpm_step(wave, n_map, dz, energy, ps):
+    """Naive WPM step (propagation.py:184-212): pixel p of the new wave is
+    pixel p of ifft2(fft2(wave) exp(i dz sqrt((n_p k0)^2 - k_perp^2))), one
+    full propagate per pixel.  k_perp^2 from get_frequencies(ny, nx, ps)
+    (axis 0: fftfreq(ny, ps[0]), axis 1: fftfreq(nx, ps[1]))."""
+    wave = np.asarray(wave, dtype=np.complex128)
+    ny, nx = wave.shape
+    k0 = 2 * np.pi / energy2wavelength(energy)
+    Fy, Fx = get_frequencies(ny, nx, ps)
+    k_perp2 = (2 * np.pi * Fx) ** 2 + (2 * np.pi * Fy) ** 2
+    Ek = _fft2(wave)
+    n_flat = np.asarray(n_map, dtype=np.float64).reshape(-1)
+    out = np.empty(ny * nx, np.complex128)
+    for p in range(n_flat.size):
+        out[p] = wpm_propagation_kernel(Ek, n_flat[p], k0, k_perp2, dz).reshape(-1)[p]
+    return out.reshape(ny, nx)
 
 
 # ---------------------------------------------------------------------------
@@ -400,6 +423,41 @@ def downsample_to_max_angle(pattern, sampling, wavelength, max_angle_mrad, parit
     y0 = cy - new_ny // 2
     x0 = cx - new_nx // 2
     return arr[..., y0:y0 + new_ny, x0:x0 + new_nx]
+
+
+# ---------------------------------------------------------------------------
+# propagation.py:609-652 (1D helpers)
+# ---------------------------------------------------------------------------
+def get_kx_1d(n, dx):
+    """2 pi fftfreq(n, dx) (propagation.py:609-614)."""
+    return 2 * np.pi * np.fft.fftfreq(n, d=dx)
+
+
+def fresnel_kernel_1d(kx_sq, k0, dy):
+    """exp(-i kx^2 dy / (2 k0)) (propagation.py:617-619)."""
+    return np.exp(-1j * np.asarray(kx_sq) * dy / (2 * k0))
+
+
+def angular_spectrum_kernel_1d(kx_sq, k0, dy):
+    """exp(i dy sqrt(k0^2 - kx^2)), complex sqrt (propagation.py:622-626)."""
+    kz = np.sqrt(np.asarray(k0 ** 2 - np.asarray(kx_sq), dtype=np.complex128))
+    return np.exp(1j * dy * kz)
+
+
+def propagate_1d(psi, H):
+    """ifft(fft(psi) H) along the last axis (propagation.py:629-633)."""
+    return np.fft.ifft(np.fft.fft(np.asarray(psi, dtype=np.complex128), axis=-1) * H, axis=-1)
+
+
+def wpm_kernel_1d(psi_k, n_val, k0, kx_sq, dy):
+    """ifft(psi_k exp(i dy sqrt((n k0)^2 - kx^2))) (propagation.py:636-649)."""
+    kz = np.sqrt(np.asarray((n_val * k0) ** 2 - np.asarray(kx_sq), dtype=np.complex128))
+    return np.fft.ifft(np.asarray(psi_k) * np.exp(1j * dy * kz))
+
+
+def wpm_kernel_1d_vmap(psi_k, n_vals, k0, kx_sq, dy):
+    """wpm_kernel_1d over an array of refractive indices (propagation.py:652)."""
+    return np.stack([wpm_kernel_1d(psi_k, n, k0, kx_sq, dy) for n in np.asarray(n_vals)])
 
 
 def rel_l2(a, b) -> float:

@@ -215,6 +215,28 @@ def make(ref_root: str, out: str):
     g["crop_odd"] = np.asarray(ref.downsample_to_max_angle(pat, (0.1, 0.1), 0.025, 40.0))
     g["crop_even"] = np.asarray(ref.downsample_to_max_angle(pat, (0.1, 0.12), 0.025, 50.0, parity="even"))
 
+    # --- naive per-pixel WPM step (small grid: one propagate per pixel) ------
+    ny, nx, ps, dz, E = 16, 24, 0.05, 2.04, 300e3
+    Vn = _gauss_stack(rng, 1, ny, nx, ps, 3, 80.0, 0.2)[0] / dz
+    wave = _probe(ny, nx, ps, ref.energy2wavelength(E), 0.05, rng)
+    nmap = ref.electron_refractive_index(Vn, E)
+    g.update(naive_wave=wave, naive_n=np.asarray(nmap), naive_meta=np.array([ny, nx, ps, dz, E]),
+             naive_out=np.asarray(ref.wpm_step(wave, nmap, dz, E, (ps, ps))))
+
+    # --- 1D helpers (k0 small enough that the AS kernel has evanescent parts) --
+    n1, dx1, dy1, k01 = 64, 0.35, 1.7, 7.0
+    kx = np.asarray(ref.get_kx_1d(n1, dx1))
+    psi1 = rng.normal(size=(3, n1)) + 1j * rng.normal(size=(3, n1))
+    Hf = np.asarray(ref.fresnel_kernel_1d(kx ** 2, k01, dy1))
+    Ha = np.asarray(ref.angular_spectrum_kernel_1d(kx ** 2, k01, dy1))
+    psik = np.fft.fft(psi1[0])
+    nv = np.array([1.0, 1.2, 1.5, 2.0])
+    g.update(l1_meta=np.array([n1, dx1, dy1, k01]), l1_kx=kx, l1_psi=psi1, l1_Hf=Hf, l1_Ha=Ha,
+             l1_prop_f=np.stack([np.asarray(ref.propagate_1d(p, Hf)) for p in psi1]),
+             l1_prop_a=np.stack([np.asarray(ref.propagate_1d(p, Ha)) for p in psi1]),
+             l1_nvals=nv, l1_wpm1=np.asarray(ref.wpm_kernel_1d(psik, 1.3, k01, kx ** 2, dy1)),
+             l1_wpmv=np.asarray(ref.wpm_kernel_1d_vmap(psik, nv, k01, kx ** 2, dy1)))
+
     np.savez_compressed(out, **g)
     print(f"wrote {out} ({os.path.getsize(out)} bytes, {len(g)} arrays)")
 

@@ -96,3 +96,22 @@ def test_detector_crop(golden):
     assert np.array_equal(O.downsample_to_max_angle(golden["crop_in"], (0.1, 0.1), 0.025, 40.0), golden["crop_odd"])
     assert np.array_equal(O.downsample_to_max_angle(golden["crop_in"], (0.1, 0.12), 0.025, 50.0, parity="even"),
                           golden["crop_even"])
+
+
+def test_naive_wpm_step(golden):
+    ny, nx, ps, dz, E = golden["naive_meta"]
+    out = O.wpm_step(golden["naive_wave"], golden["naive_n"], dz, E, (ps, ps))
+    assert O.rel_l2(out, golden["naive_out"]) < 1e-12
+
+
+def test_1d_helpers(golden):
+    n, dx, dy, k0 = golden["l1_meta"]
+    kx = O.get_kx_1d(int(n), dx)
+    assert np.array_equal(kx, golden["l1_kx"])
+    assert O.rel_l2(O.fresnel_kernel_1d(kx ** 2, k0, dy), golden["l1_Hf"]) < 1e-14
+    assert O.rel_l2(O.angular_spectrum_kernel_1d(kx ** 2, k0, dy), golden["l1_Ha"]) < 1e-14
+    assert O.rel_l2(O.propagate_1d(golden["l1_psi"], golden["l1_Hf"]), golden["l1_prop_f"]) < 1e-13
+    assert O.rel_l2(O.propagate_1d(golden["l1_psi"], golden["l1_Ha"]), golden["l1_prop_a"]) < 1e-13
+    psik = np.fft.fft(golden["l1_psi"][0])
+    assert O.rel_l2(O.wpm_kernel_1d(psik, 1.3, k0, kx ** 2, dy), golden["l1_wpm1"]) < 1e-13
+    assert O.rel_l2(O.wpm_kernel_1d_vmap(psik, golden["l1_nvals"], k0, kx ** 2, dy), golden["l1_wpmv"]) < 1e-13

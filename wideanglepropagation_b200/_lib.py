@@ -36,6 +36,10 @@ SIGNATURES = {
     "wap_plan_destroy": (_I, [_P]),
     "wap_plan_set_config": (_I, [_P, _I, _I, _I]),
     "wap_plan_set_detector": (_I, [_P, _I, _I, _I, _I]),
+    "wap_line_transfer": (_I, [_I, _I, _P, _D, _D, _P, _P]),
+    "wap_line_propagate": (_I, [_I, _I, _P, _P, _P, _I, _P, _P]),
+    "wap_line_wpm": (_I, [_I, _I, _P, _P, _D, _P, _D, _P, _P]),
+    "wap_wpm_naive_step": (_I, [_I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _P]),
     "wap_plan_get_config": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_transfer_function": (_I, [_I, _I, _I, _D, _D, _D, _D, _P, _I, _P, _P]),
     "wap_multislice_fwd": (_I, [_P, _P, _I, _I, _P, _P, _I, _I, _P, _P, _P, _D, _D, _P, _P, _P, _P]),
