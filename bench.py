@@ -286,12 +286,15 @@ def main():
         extras.update(_grad_ratio(args))
         extras.update(_err_vs_fp64(classes, classes_host))
         extras.update(_lines())
+        extras.update(_potential_builder())
 
     # --- e2e through the public API from pinned host buffers ------------------
     e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
     if not args.no_extras:
         # the same with a 50 mrad detector: the crop is fused into the last column pass
         extras["e2e_detector_50mrad"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=50.0)
+        # the same from atom lists: the potential is built on the device
+        extras["e2e_from_atoms"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, from_atoms=True)
 
     cpu = None
     if rank == 0 and not args.no_extras:
@@ -480,6 +483,37 @@ def _peak_hbm():
     return 6650.0, "fallback"
 
 
+def _potential_builder():
+    """Device potential builder on the C2 configuration (1024^2 diamond [100],
+    100 slices: 419 MB of float32 written) vs the host NumPy builder (4 slices,
+    scaled)."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    import wideanglepropagation_b200.synthetic as S
+    n, N, ps, dz = 1024, 100, 0.05, 1.3575
+    pos, sl = S.lattice_atoms(np.random.default_rng(0), N, n, n, ps, 5.43, S.DIAMOND_LAYERS, 0.08)
+    for _ in range(2):
+        V = wap.gaussian_potential(N, n, n, ps, pos, sl, 25.0, 0.25, scale=1 / dz)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    s.record()
+    for _ in range(reps):
+        V = wap.gaussian_potential(N, n, n, ps, pos, sl, 25.0, 0.25, scale=1 / dz)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / reps
+    del V
+    t0 = time.perf_counter()
+    S.lattice_stack(np.random.default_rng(0), 4, n, n, ps, 5.43, S.DIAMOND_LAYERS, 25.0, 0.25, 0.08)
+    host_ms = (time.perf_counter() - t0) * 1e3 * N / 4
+    gbs = 4.0 * N * n * n / (ms / 1e3) / 1e9
+    peak, src = _peak_hbm()
+    return {"potential_builder_c2": {"ms": ms, "atoms": int(pos.shape[0]), "written_gbs": gbs, "peak_gbs": peak,
+                                     "peak_source": src, "frac": gbs / peak, "host_numpy_ms": host_ms,
+                                     "note": "includes the atom-list upload (pageable) in each call"}}
+
+
 def _lines():
     """1D helpers: propagate_1d over 65536 lines of 2048 points (1 GiB in,
     1 GiB out: HBM-bound, 16 B per point) and the naive per-pixel WPM step on
@@ -536,26 +570,43 @@ def _err_vs_fp64(classes, classes_host):
     return {"err_vs_fp64": errs}
 
 
-def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None):
+def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None, from_atoms=False):
     """The headline workload through simulate_fresnel_as from pinned host
     buffers; with ``max_angle`` (mrad) the patterns come back cropped to that
-    detector window (the crop fused into the last column pass)."""
+    detector window (the crop fused into the last column pass); with
+    ``from_atoms`` each step uploads the atom lists instead of the potential
+    and builds the potential on the device (gaussian_potential)."""
     import torch
     import wideanglepropagation_b200 as wap
+    import wideanglepropagation_b200.synthetic as S
     host = []
-    for w in classes_host:
+    atoms = []
+    for ci, w in enumerate(classes_host):
         V = torch.from_numpy(w.potential).pin_memory()
+        if from_atoms:
+            D, N = w.potential.shape[:2]
+            side = int(round((w.n_probes // D) ** 0.5))
+            pos, rows = S.batched_scan_class_atoms(ci, w.ny, N, side, D)   # the seeds of batched_scan(0)
+            atoms.append((pos, rows, D, N))
         H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
         win = wap.detector_window((w.ny, w.nx), (w.ps, w.ps), w.energy, max_angle) if max_angle else None
         shape = (w.n_probes, win[2], win[3]) if win else (w.n_probes, w.ny, w.nx)
         host.append((w, V, torch.from_numpy(w.probe).pin_memory(), torch.from_numpy(w.positions).pin_memory(),
                      torch.from_numpy(w.draw_of_probe).pin_memory(), H,
                      torch.empty(shape, dtype=torch.float32).pin_memory()))
-    h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
+    if from_atoms:
+        h2d = sum(p.nbytes // 2 * 3 + (N * D + 1) * 4 for p, _, D, N in atoms)   # (M, 3) float64 + offsets
+        h2d += sum(p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, _, p, q, d, _, _ in host)
+    else:
+        h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
     d2h = sum(o.numel() * 4 for *_, o in host)
 
     def step():
-        for w, V, p, q, d, H, out in host:
+        for i, (w, V, p, q, d, H, out) in enumerate(host):
+            if from_atoms:
+                pos, rows, D, N = atoms[i]
+                V = wap.gaussian_potential(D * N, w.ny, w.nx, w.ps, pos, rows, 25.0, 0.25,
+                                           scale=1 / w.dz).view(D, N, w.ny, w.nx)
             _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False,
                                                max_angle=max_angle, sampling=(w.ps, w.ps))
             out.copy_(dp, non_blocking=True)
@@ -574,6 +625,8 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None
     total = sum(w.n_probes * w.n_slices for w in classes_host)
     api = "simulate_fresnel_as(positions=, draw=)" if not max_angle else \
         f"simulate_fresnel_as(positions=, draw=, max_angle={max_angle:g}, sampling=)"
+    if from_atoms:
+        api = "gaussian_potential(atoms) + " + api
     return {"value": total * world / (ms / 1e3), "unit": "slice-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": api}
 

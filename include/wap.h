@@ -126,6 +126,22 @@ int wap_line_wpm(int n, int n_refs, const float* psi_k, const double* n_vals, do
 int wap_wpm_naive_step(int ny, int nx, const double* wave, const double* n_map, double dz, double energy,
                        double ps0, double ps1, double* out, double* work, void* stream);
 
+/* Projected potential of Gaussian atoms, built on the device:
+ *   V[s, y, x] = scale * sum_{a in slice s} amp_a exp(-(dy^2 + dx^2) / (2 sigma^2))
+ * with dy, dx the periodic distances ((p - c + L/2) mod L) - L/2 of pixel
+ * (y ps_y, x ps_x) to atom a on the (ny ps_y) x (nx ps_x) box.
+ *   atoms        (n_atoms, 3) float64: y, x (A), amplitude (V A), grouped by slice
+ *   slice_start  (n_slices + 1) int32 offsets: slice s holds atoms
+ *                slice_start[s] .. slice_start[s+1]-1
+ *   scale        e.g. 1/dz to pass the potential in volts
+ *   V            (n_slices, ny, nx) float32 out
+ * Atoms farther than 7 sigma from a pixel are skipped (< 2.3e-11 of a peak).
+ * Replaces the host-side potential construction that precedes the multislice
+ * (get_abtem_transmit, propagation.py:286-299, builds abTEM potentials on the
+ * host; the benchmark configurations use this Gaussian-atom model). */
+int wap_gaussian_potential(int n_slices, int ny, int nx, double ps_y, double ps_x, const double* atoms,
+                           const int32_t* slice_start, double sigma, double scale, float* V, void* stream);
+
 /* WPM adaptive-binning multislice forward, propagation.py:358-387 with the
  * step of propagation.py:215-256 (n_bins reference indices spaced
  * n_min + (n_max - n_min) t^power_spacing per slice, smoothstep blend of the

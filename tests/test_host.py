@@ -94,3 +94,12 @@ def test_no_cpu_fallback():
                                 np.ones((64, 64), np.complex64), 1.0, 2e5)
     with pytest.raises(RuntimeError, match="no CPU path"):
         wap.fresnel_propagation_kernel(64, 64, (0.1, 0.1), 1.0, 2e5)
+
+
+def test_atom_lists_reproduce_the_host_potentials():
+    """The atom lists behind the synthetic workloads give the same potentials
+    (the device builder is fed these lists)."""
+    w = synthetic.batched_scan_class(3, 64, 5, 2, 2)
+    pos, rows = synthetic.batched_scan_class_atoms(3, 64, 5, 2, 2)
+    V = np.stack([synthetic.gaussian_slice(64, 64, 0.05, pos[rows == r], 25.0, 0.25) for r in range(10)])
+    assert np.allclose(V.reshape(2, 5, 64, 64) / 1.3575, w.potential, rtol=1e-6, atol=1e-6 * np.abs(V).max())

@@ -53,6 +53,22 @@ def _release(key, h):
         _pool.setdefault(key, []).append(h)
 
 
+class _Lease:
+    """A pooled gradient scan held by one forward: returned to the pool by
+    its backward, or when the graph is freed without a backward."""
+
+    def __init__(self, key, h):
+        self.key, self.h, self.done = key, h, False
+
+    def release(self):
+        if not self.done:
+            self.done = True
+            _release(self.key, self.h)
+
+    def __del__(self):
+        self.release()
+
+
 class MultisliceFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every, det):
@@ -69,10 +85,13 @@ class MultisliceFunction(torch.autograd.Function):
             key = (torch.cuda.current_device(), ny, N, Vc.shape[0], B, k)
             h = _acquire(key, scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp, det), k)
             _lib.check(_lib.lib().wap_scan_run(h, _stream()))
-            ctx.scan = (key, h)
-            # everything the scan reads in the backward must outlive it
-            ctx.keep = (Vc, psi, pos, dr, Hc, Hl, exit_wave, dp)
-            ctx.save_for_backward(Vc)
+            ctx.scan = _Lease(key, h)
+            # everything the scan reads in the backward must outlive it.  The
+            # exit wave is an output: it goes through save_for_backward (a
+            # plain attribute would tie output -> graph -> ctx -> output in a
+            # cycle that only the garbage collector frees)
+            ctx.keep = (psi, pos, dr, Hc, Hl)
+            ctx.save_for_backward(Vc, exit_wave)
             ctx.meta = (B, N, ny, nx, float(dz), float(energy), k, dr is not None, V.shape, batched, det)
             if not batched:
                 return exit_wave[0], dp[0]
@@ -99,8 +118,9 @@ class MultisliceFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g_exit, g_dp):
         if ctx.scan is not None:
-            key, h = ctx.scan
-            (Vc,) = ctx.saved_tensors
+            lease = ctx.scan
+            h = lease.h
+            Vc, _ = ctx.saved_tensors
             B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta
             try:
                 if g_exit is None and g_dp is not None:
@@ -109,10 +129,10 @@ class MultisliceFunction(torch.autograd.Function):
                     _lib.check(_lib.lib().wap_scan_grad_backward(h, _ptr(g), _ptr(grad_V), _stream()))
                     return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
             finally:
-                _release(key, h)
+                lease.release()
             # a loss on the exit wave: the per-pass adjoint below needs its own checkpoints
-            Vc2, psi, pos, dr, Hc, Hl, _, _ = ctx.keep
-            return _per_pass_backward(Vc2, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp,
+            psi, pos, dr, Hc, Hl = ctx.keep
+            return _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp,
                                       det)
         Vc, Hc, Hl, exit_wave, ckpt, dr = ctx.saved_tensors
         B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta

@@ -421,7 +421,7 @@ ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo) {
   c.ny = p->ny;
   c.nx = p->nx;
   c.seed_scale = (float)((double)p->ny * p->nx);
-  c.det = p->det;
+  c.det = p->det.resolved(p->ny, p->nx);
   return c;
 }
 

@@ -10,19 +10,13 @@
 namespace wap {
 // Detector window of a diffraction pattern: rows y0 .. y0+ny-1 and columns
 // x0 .. x0+nx-1 of the fftshifted |fft2(psi)|^2 - the centre crop of
-// downsample_to_max_angle (propagation.py:424-439).  ny == 0: the whole grid.
+// downsample_to_max_angle (propagation.py:424-439).  A plan keeps ny == 0 for
+// "the whole grid"; kernels always receive a resolved window.
 struct Detector {
   int y0 = 0, x0 = 0, ny = 0, nx = 0;
-  // pixels of one probe's pattern on a gy x gx grid
-  __host__ __device__ long long plane(int gy, int gx) const {
-    return ny == 0 ? (long long)gy * gx : (long long)ny * nx;
-  }
-  // index of the fftshifted pixel (sy, sx) in one probe's pattern, -1 outside
-  __host__ __device__ long long index(int sy, int sx, int gx) const {
-    if (ny == 0) return (long long)sy * gx + sx;
-    const int ry = sy - y0, rx = sx - x0;
-    return ((unsigned)ry < (unsigned)ny && (unsigned)rx < (unsigned)nx) ? (long long)ry * nx + rx : -1LL;
-  }
+  __host__ __device__ Detector resolved(int gy, int gx) const { return ny == 0 ? Detector{0, 0, gy, gx} : *this; }
+  // pixels of one probe's pattern
+  __host__ __device__ long long plane() const { return (long long)ny * nx; }
 };
 }  // namespace wap
 

@@ -140,6 +140,7 @@ extern "C" int wap_multislice_fwd_noalloc(const float* V, int n_slices, int ny, 
   c.ny = ny;
   c.nx = nx;
   c.dp = dp;
+  c.det = Detector{0, 0, ny, nx};   // the whole pattern
   int col_w = 16;
   while (col_w > 1 && (col_w * (ny / col_e) > kColThreads || (size_t)ny * col_w * 8 > 96 * 1024)) col_w >>= 1;
   if (col_w > nx) col_w = nx;

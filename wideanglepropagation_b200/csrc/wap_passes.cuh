@@ -331,14 +331,17 @@ col_pass_kernel(const ColArgs a) {
 
   // fftshift of (ky, kx) for dp / g
   const int sx = (col + (nx >> 1)) & (nx - 1);
+  // position of this column in the detector window (rows are tested per element)
+  const int drx = sx - a.det.x0;
+  const bool dcol = (unsigned)drx < (unsigned)a.det.nx;
   if constexpr (SEED) {
-    const float* gp = a.g + (long long)b * a.det.plane(NY, nx);
+    const float* gp = a.g + (long long)b * a.det.plane() + drx;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int ky = t + T * e;
-      const int sy = (ky + (NY >> 1)) & (NY - 1);
-      const long long gi = a.det.index(sy, sx, nx);
-      v[e] = (a.g && gi >= 0) ? cscale(v[e], a.seed_scale * __ldg(gp + gi)) : make_float2(0.f, 0.f);
+      const int ry = ((ky + (NY >> 1)) & (NY - 1)) - a.det.y0;
+      const bool in = a.g && dcol && (unsigned)ry < (unsigned)a.det.ny;
+      v[e] = in ? cscale(v[e], a.seed_scale * __ldg(gp + ry * a.det.nx)) : make_float2(0.f, 0.f);
     }
     if (a.seed2) {
       float2 u[E];
@@ -380,13 +383,12 @@ col_pass_kernel(const ColArgs a) {
   }
 
   if (f & COL_DP) {
-    float* dp = a.dp + (long long)b * a.det.plane(NY, nx);
+    float* dp = a.dp + (long long)b * a.det.plane() + drx;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int ky = t + T * e;
-      const int sy = (ky + (NY >> 1)) & (NY - 1);
-      const long long di = a.det.index(sy, sx, nx);
-      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      const int ry = ((ky + (NY >> 1)) & (NY - 1)) - a.det.y0;
+      if (dcol && (unsigned)ry < (unsigned)a.det.ny) __stcs(dp + ry * a.det.nx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
     if (f & COL_NO_H) return;  // pure diffraction epilogue: no inverse transform
   }
@@ -521,13 +523,13 @@ wpm_col_kernel(const WpmColArgs a) {
   fft<NY, E, false>(v, t, xs, tw);
 
   if (a.dp_mode) {
-    float* dp = a.dp + (long long)b * a.det.plane(NY, nx);
-    const int sx = (col + (nx >> 1)) & (nx - 1);
+    const int drx = ((col + (nx >> 1)) & (nx - 1)) - a.det.x0;
+    if ((unsigned)drx >= (unsigned)a.det.nx) return;   // column outside the detector window
+    float* dp = a.dp + (long long)b * a.det.plane() + drx;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const int sy = (t + T * e + (NY >> 1)) & (NY - 1);
-      const long long di = a.det.index(sy, sx, nx);
-      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      const int ry = ((t + T * e + (NY >> 1)) & (NY - 1)) - a.det.y0;
+      if ((unsigned)ry < (unsigned)a.det.ny) __stcs(dp + ry * a.det.nx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
     return;
   }

@@ -116,8 +116,7 @@ struct SchedClass {
   const float2* ttab;           // (draws, N, n, n)  t / (n n)
   long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
-  float* dp;                    // (B, n, n), (B, detector window) or null
-  Detector det;                 // window of dp and g
+  float* dp;                    // (B, n, n) or null (a windowed class: the scan's full-grid scratch)
   // gradient buffers
   float2* lam;                  // (B, n, n) adjoint state
   float2* work;                 // (B, n, n) recompute buffer
@@ -126,7 +125,7 @@ struct SchedClass {
   int ckpt_n, seg_n;            // slots per probe
   int ckpt_k;                   // gradient scans: checkpoint every ckpt_k slices (0: none)
   int seg_first;                // first slice of the last segment (kept by the forward)
-  const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp
+  const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp (full grid)
   float* grad;                  // (draws, N, n, n) probe sums of Re(conj(lambda_a) i a_s)
   float ri_a, ri_inv_den, kphase, e_plus_e0;
   const float4* tw;             // twiddles for (n, E) in global memory
@@ -483,12 +482,11 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     if (type == ST_SEED_COL) {
       // lambda seed: n^2 g Z with g = dL/d(dp) at the fftshifted position
       // (zero outside the detector window)
-      const float* gp = c.g + (long long)k.b * c.det.plane(N, N);
+      const float* gp = c.g + (long long)k.b * plane;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int sy = (t + T * e + (N >> 1)) & (N - 1);
-        const long long gi = c.det.index(sy, sx, N);
-        v[e] = gi >= 0 ? cscale(v[e], c.inv_scale * __ldg(gp + gi)) : make_float2(0.f, 0.f);
+        v[e] = cscale(v[e], c.inv_scale * __ldg(gp + (long long)sy * N + sx));
       }
     }
   }
@@ -508,12 +506,11 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     }
   }
   if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
-    float* dp = c.dp + (long long)k.b * c.det.plane(N, N);
+    float* dp = c.dp + (long long)k.b * plane;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int sy = (t + T * e + (N >> 1)) & (N - 1);
-      const long long di = c.det.index(sy, sx, N);
-      if (di >= 0) __stcs(dp + di, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
+      __stcs(dp + (long long)sy * N + sx, fmaf(v[e].x, v[e].x, v[e].y * v[e].y));
     }
   }
   fft<N, E, true>(v, t, xs, tw);
@@ -771,6 +768,32 @@ static __global__ void __launch_bounds__(256) grad_finalize_kernel(const float* 
   }
 }
 
+// Detector windows of the scheduler.  An inlined window test in the persistent
+// kernel's pattern store and adjoint seed raises the register pressure of
+// every tile body (measured on B200: +1.2 % on the batched scan, +6 % on the
+// adjoint sweep), so a windowed class runs on a full-grid scratch pattern and
+// these two passes move the window in and out (about 0.1 % of a step).
+static __global__ void __launch_bounds__(256) crop_window_kernel(const float* __restrict__ full,
+                                                          float* __restrict__ dp, long long total, int n, Detector d) {
+  const long long per = (long long)d.ny * d.nx;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long b = i / per;
+    const int r = (int)(i - b * per), ry = r / d.nx, rx = r - ry * d.nx;
+    dp[i] = __ldcs(full + (b * n + d.y0 + ry) * n + d.x0 + rx);
+  }
+}
+
+static __global__ void __launch_bounds__(256) scatter_window_kernel(const float* __restrict__ g,
+                                                             float* __restrict__ full, long long total, int n,
+                                                             Detector d) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long b = i / ((long long)n * n);
+    const int r = (int)(i - b * n * n), y = r / n - d.y0, x = r % n - d.x0;
+    const bool in = (unsigned)y < (unsigned)d.ny && (unsigned)x < (unsigned)d.nx;
+    full[i] = in ? __ldg(g + (b * d.ny + y) * d.nx + x) : 0.0f;
+  }
+}
+
 }  // namespace wap
 
 // ---------------------------------------------------------------------------
@@ -827,6 +850,8 @@ struct wap_scan {
   int grid_bwd = 0;                 // backward launch (two staging buffers with kPsiStage2)
   size_t smem_bwd = 0;
   int psi_mode = kPsiSplit;         // how the backward's adjoint rows get psi_s
+  std::vector<Detector> det;        // per class: diffraction-pattern window (the whole grid: no window)
+  std::vector<float*> d_dpfull;     // per windowed class: (B, n, n) full-grid pattern / seed scratch
   float* d_gsum = nullptr;          // (draws, N, n, n) probe sums of the adjoint sweep
   int ckpt_every = 0;
   std::vector<float4*> d_tw;
@@ -864,16 +889,19 @@ static void scan_free(wap_scan* s) {
   for (auto p : s->d_ttab) cudaFree(p);
   for (auto p : s->d_hq) cudaFree(p);
   for (auto p : s->d_extra) cudaFree(p);
+  for (auto p : s->d_dpfull) cudaFree(p);
   cudaFree(s->d_gsum);
   delete s;
 }
 
 static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n == 1024; }
 
+static bool windowed(const Detector& d, int n) { return d.ny != n || d.nx != n; }
+
 // detector window of a class's diffraction patterns (0 x 0: the whole grid)
 static int class_detector(const wap_scan_class& c, int ci, Detector* d) {
   if (c.det_ny == 0 && c.det_nx == 0) {
-    *d = Detector{};
+    *d = Detector{0, 0, c.n, c.n};
     return WAP_OK;
   }
   if (c.det_ny < 1 || c.det_nx < 1 || c.det_y0 < 0 || c.det_x0 < 0 || c.det_y0 + c.det_ny > c.n ||
@@ -881,6 +909,27 @@ static int class_detector(const wap_scan_class& c, int ci, Detector* d) {
     return fail(WAP_ERR_ARG, "scan class %d: detector window rows %d+%d, columns %d+%d outside the %d x %d grid", ci,
                 c.det_y0, c.det_ny, c.det_x0, c.det_nx, c.n, c.n);
   *d = Detector{c.det_y0, c.det_x0, c.det_ny, c.det_nx};
+  return WAP_OK;
+}
+
+// Record class ci's window and point its pattern at the user's buffer, or at
+// the class's full-grid scratch (allocated the first time a window is set).
+static int bind_detector(wap_scan* s, const wap_scan_class& c, int ci) {
+  if ((int)s->det.size() < ci + 1) {
+    s->det.resize(ci + 1);
+    s->d_dpfull.resize(ci + 1, nullptr);
+  }
+  int rc = class_detector(c, ci, &s->det[ci]);
+  if (rc) return rc;
+  SchedClass& sc = s->params.cls[ci];
+  sc.dp = c.dp;
+  if (c.dp && windowed(s->det[ci], c.n)) {
+    if (!s->d_dpfull[ci]) {
+      cudaError_t e = cudaMalloc(&s->d_dpfull[ci], (size_t)c.n_probes * c.n * c.n * sizeof(float));
+      if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(full-grid pattern scratch)");
+    }
+    sc.dp = s->d_dpfull[ci];
+  }
   return WAP_OK;
 }
 
@@ -1119,7 +1168,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     sc.draw = c.draw;
     sc.V = c.V;
     sc.dp = c.dp;
-    if ((rc0 = class_detector(c, ci, &sc.det))) return rc0;
+    if ((rc0 = bind_detector(s, c, ci))) return rc0;
     sc.vstride = (long long)c.n_slices * n * n;
     sc.scale = (float)(1.0 / ((double)n * n));
     sc.inv_scale = (float)((double)n * n);
@@ -1242,6 +1291,16 @@ static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   if (backward) {
     params.stage2 = s->psi_mode;
     params.cls[0].grad = s->d_gsum;
+    if (windowed(s->det[0], s->cls[0].n)) {
+      // the seed reads a full-grid dL/d(dp): zero outside the window
+      const wap_scan_class& c = s->cls[0];
+      const long long total = (long long)c.n_probes * c.n * c.n;
+      count_launch();
+      scatter_window_kernel<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, st>>>(
+          s->params.cls[0].g, s->d_dpfull[0], total, c.n, s->det[0]);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scatter_window_kernel");
+      params.cls[0].g = s->d_dpfull[0];
+    }
     if ((e = cudaMemsetAsync(s->d_gsum, 0, s->ttab_elems[0] * sizeof(float), st)) != cudaSuccess)
       return cuda_fail(e, "gradient sums reset");
     grid = s->grid_bwd;
@@ -1281,6 +1340,17 @@ static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   (backward ? s->kernel_bwd : s->kernel)<<<grid, kBlockThreads, smem, st>>>(params);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scan_kernel");
   prof_end(tok, st, bytes);
+  if (!backward) {
+    for (int ci = 0; ci < s->n_classes; ++ci) {
+      const wap_scan_class& c = s->cls[ci];
+      if (!c.dp || !windowed(s->det[ci], c.n)) continue;
+      const long long total = (long long)c.n_probes * s->det[ci].ny * s->det[ci].nx;
+      count_launch();
+      crop_window_kernel<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, st>>>(
+          s->d_dpfull[ci], c.dp, total, c.n, s->det[ci]);
+      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "crop_window_kernel");
+    }
+  }
   if (backward) {
     const Physics& ph = s->phys[0];
     const long long n4 = (long long)s->ttab_elems[0] / 4;
@@ -1353,7 +1423,7 @@ int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
     sc.draw = c.draw;
     sc.V = c.V;
     sc.dp = c.dp;
-    if ((rc = class_detector(c, ci, &sc.det))) return rc;
+    if ((rc = bind_detector(s, c, ci))) return rc;
     s->cls[ci] = c;
     s->phys[ci] = physics(c.energy, c.dz);
     const Physics& ph = s->phys[ci];

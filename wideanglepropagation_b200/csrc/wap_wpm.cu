@@ -122,7 +122,7 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
   c.n_slices = n_slices;
   c.k02 = (float)(ph.k0 * ph.k0);
   c.dz = (float)dz;
-  c.det = p->det;
+  c.det = p->det.resolved(p->ny, p->nx);
 
   WpmRowArgs w{};
   w.psi = reinterpret_cast<float2*>(exit);

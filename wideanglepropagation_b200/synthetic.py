@@ -36,12 +36,19 @@ def gaussian_slice(ny, nx, ps, centres_yx, amp, sigma):
     return (amp * gy).T @ gx
 
 
+def random_gaussian_atoms(rng, n_slices, ny, nx, ps, n_atoms=30):
+    """Atom list of ``random_gaussian_stack``: (positions (M, 2) in A, slice of each atom)."""
+    L = np.array([ny * ps, nx * ps])
+    pos = np.concatenate([rng.uniform(0, 1, (n_atoms, 2)) * L for _ in range(n_slices)])
+    return pos, np.repeat(np.arange(n_slices), n_atoms)
+
+
 def random_gaussian_stack(rng, n_slices, ny, nx, ps, n_atoms=30, amp=20.0, sigma=0.3):
     """Each slice: ``n_atoms`` Gaussians at seed-uniform centres (V*A)."""
+    pos, sl = random_gaussian_atoms(rng, n_slices, ny, nx, ps, n_atoms)
     out = np.empty((n_slices, ny, nx), np.float64)
-    L = np.array([ny * ps, nx * ps])
     for s in range(n_slices):
-        out[s] = gaussian_slice(ny, nx, ps, rng.uniform(0, 1, (n_atoms, 2)) * L, amp, sigma)
+        out[s] = gaussian_slice(ny, nx, ps, pos[sl == s], amp, sigma)
     return out
 
 
@@ -52,15 +59,15 @@ DIAMOND_LAYERS = [[(0, 0), (0.5, 0.5)], [(0.25, 0.25), (0.75, 0.75)],
 FCC_LAYERS = [[(0, 0), (0.5, 0.5)], [(0.5, 0), (0, 0.5)]]
 
 
-def lattice_stack(rng, n_slices, ny, nx, ps, a, layers, amp, sigma, jitter):
-    """Per-slice projected potential of a cubic lattice seen along [100].
+def lattice_atoms(rng, n_slices, ny, nx, ps, a, layers, jitter):
+    """Atom list of ``lattice_stack``: (positions (M, 2) in A, slice of each atom).
 
     Slice s holds the atomic layer ``layers[s % len(layers)]``; every atom
     gets an independent N(0, jitter) in-plane displacement (frozen phonon).
     """
     Ly, Lx = ny * ps, nx * ps
     ncy, ncx = int(math.ceil(Ly / a)), int(math.ceil(Lx / a))
-    out = np.empty((n_slices, ny, nx), np.float64)
+    all_pos, all_sl = [], []
     for s in range(n_slices):
         frac = np.asarray(layers[s % len(layers)], dtype=np.float64)
         iy, ix = np.meshgrid(np.arange(ncy), np.arange(ncx), indexing="ij")
@@ -68,7 +75,18 @@ def lattice_stack(rng, n_slices, ny, nx, ps, a, layers, amp, sigma, jitter):
         pos = (cells[:, None, :] + frac[None, :, :]).reshape(-1, 2) * a
         pos = pos[(pos[:, 0] < Ly) & (pos[:, 1] < Lx)]
         pos = pos + rng.normal(0, jitter, pos.shape)
-        out[s] = gaussian_slice(ny, nx, ps, pos, amp, sigma)
+        all_pos.append(pos)
+        all_sl.append(np.full(pos.shape[0], s))
+    return np.concatenate(all_pos), np.concatenate(all_sl)
+
+
+def lattice_stack(rng, n_slices, ny, nx, ps, a, layers, amp, sigma, jitter):
+    """Per-slice projected potential of a cubic lattice seen along [100]
+    (the atoms of ``lattice_atoms``, Gaussians of ``amp`` V*A and ``sigma`` A)."""
+    pos, sl = lattice_atoms(rng, n_slices, ny, nx, ps, a, layers, jitter)
+    out = np.empty((n_slices, ny, nx), np.float64)
+    for s in range(n_slices):
+        out[s] = gaussian_slice(ny, nx, ps, pos[sl == s], amp, sigma)
     return out
 
 
@@ -179,6 +197,20 @@ def batched_scan_class(seed, n, n_slices, n_side, n_draws):
     return Workload(f"scan_{n}_N{n_slices}_B{positions.shape[0]}", n, n, ps, n_slices, dz, E,
                     V, probe, positions=positions.astype(np.int32),
                     draw_of_probe=draws, method="as")
+
+
+def batched_scan_class_atoms(seed, n, n_slices, n_side, n_draws):
+    """Atom lists behind ``batched_scan_class`` (same seed, same draws):
+    positions (M, 2) in A and the row of each atom in the (n_draws * n_slices)
+    stack of slices; the potential is these atoms as 25 V*A / 0.25 A Gaussians
+    divided by the slice thickness 1.3575 A."""
+    rng = np.random.default_rng(seed)
+    pos, rows = [], []
+    for d in range(n_draws):
+        p, s = lattice_atoms(rng, n_slices, n, n, 0.05, 5.43, DIAMOND_LAYERS, 0.08)
+        pos.append(p)
+        rows.append(s + d * n_slices)
+    return np.concatenate(pos), np.concatenate(rows)
 
 
 def batched_scan(seed=0, small=False):
