@@ -287,6 +287,7 @@ def main():
         extras.update(_err_vs_fp64(classes, classes_host))
         extras.update(_lines())
         extras.update(_potential_builder())
+        extras.update(_lippmann_schwinger())
 
     # --- e2e through the public API from pinned host buffers ------------------
     e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
@@ -512,6 +513,30 @@ def _potential_builder():
     return {"potential_builder_c2": {"ms": ms, "atoms": int(pos.shape[0]), "written_gbs": gbs, "peak_gbs": peak,
                                      "peak_source": src, "frac": gbs / peak, "host_numpy_ms": host_ms,
                                      "note": "includes the atom-list upload (pageable) in each call"}}
+
+
+def _lippmann_schwinger():
+    """Lippmann-Schwinger 2D solve of a 128^2 Gaussian-atom potential (padded
+    256^2, convolutions on 512^2) at the reference's default tolerance, on the
+    device and with the float64 oracle on the host cores."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    import wideanglepropagation_b200.synthetic as S
+    from oracle import propagation_oracle as O
+    V = S.random_gaussian_stack(np.random.default_rng(0), 1, 128, 128, 0.1, 30, 20.0, 0.3)[0] / 2.0
+    wap.solve_scattering_2d_lippmann_schwinger(V, 200e3, 0.1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    psi = wap.solve_scattering_2d_lippmann_schwinger(V, 200e3, 0.1)
+    torch.cuda.synchronize()
+    gpu_ms = (time.perf_counter() - t0) * 1e3
+    O.set_workers(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    ref = O.solve_scattering_2d_lippmann_schwinger(V, 200e3, 0.1)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    err = float(np.linalg.norm(psi.cpu().numpy() - ref) / np.linalg.norm(ref))
+    return {"lippmann_schwinger_128": {"device_ms": gpu_ms, "oracle_cpu_ms": cpu_ms, "rel_vs_oracle": err,
+                                        "note": "wall clock incl. the host kernel build; gmres_tol 1e-4, restart 70"}}
 
 
 def _lines():

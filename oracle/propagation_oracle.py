@@ -18,6 +18,8 @@ What it restates (reference file ``wide_angle_propagation/propagation.py``):
 * ``simulate_wpm`` ............................... :358-387
 * detector crop ``max_angle_gpts`` /
   ``downsample_to_max_angle`` .................... :394-439
+* Lippmann-Schwinger 2D (kernel, convolution,
+  GMRES solve) ................................... :446-602
 * 1D helpers ``get_kx_1d`` .. ``wpm_kernel_1d_vmap`` :609-652
 
 Parity pin: the reference module cannot be imported with its real
@@ -423,6 +425,79 @@ def downsample_to_max_angle(pattern, sampling, wavelength, max_angle_mrad, parit
     y0 = cy - new_ny // 2
     x0 = cx - new_nx // 2
     return arr[..., y0:y0 + new_ny, x0:x0 + new_nx]
+
+
+# ---------------------------------------------------------------------------
+# propagation.py:446-602 (Lippmann-Schwinger 2D)
+# ---------------------------------------------------------------------------
+def _greens_2d_hankel(k0, r):
+    """(i/4) H0^(1)(k0 r) (propagation.py:448-451)."""
+    from scipy.special import hankel1
+    return 0.25j * hankel1(0, k0 * r)
+
+
+def _self_weight_cell_average(k0, hx, hy, oversamp=32):
+    """Cell average of the Green's function over the singular cell (:454-461)."""
+    xs = (np.arange(oversamp) + 0.5) / oversamp * hx - 0.5 * hx
+    ys = (np.arange(oversamp) + 0.5) / oversamp * hy - 0.5 * hy
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    return _greens_2d_hankel(k0, np.sqrt(X ** 2 + Y ** 2)).mean() * (hx * hy)
+
+
+def build_lippmann_schwinger_kernel_2d(k0, hx, hy, Nx, Ny, pad_to_double=True, oversamp_self=32):
+    """FFT of the embedded Green's function kernel and the embedding shape (:464-501)."""
+    Ex, Ey = (2 * Nx, 2 * Ny) if pad_to_double else (Nx, Ny)
+    x = (np.arange(Nx) - Nx // 2) * hx
+    y = (np.arange(Ny) - Ny // 2) * hy
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    K = (hx * hy) * _greens_2d_hankel(k0, np.sqrt(X ** 2 + Y ** 2))
+    K[Nx // 2, Ny // 2] = _self_weight_cell_average(k0, hx, hy, oversamp=oversamp_self)
+    Kemb = np.zeros((Ex, Ey), dtype=np.complex128)
+    sx, sy = (Ex - Nx) // 2, (Ey - Ny) // 2
+    Kemb[sx:sx + Nx, sy:sy + Ny] = K
+    return np.fft.fftn(np.fft.ifftshift(Kemb)), (Ex, Ey)
+
+
+def apply_convolution(source, Khat, embed_shape, roi_shape):
+    """Centre-embedded FFT convolution with the kernel, cropped back (:504-514)."""
+    Ex, Ey = embed_shape
+    Nx, Ny = roi_shape
+    sx, sy = (Ex - Nx) // 2, (Ey - Ny) // 2
+    src = np.zeros((Ex, Ey), dtype=np.complex128)
+    src[sx:sx + Nx, sy:sy + Ny] = source
+    return np.fft.ifftn(Khat * np.fft.fftn(src))[sx:sx + Nx, sy:sy + Ny]
+
+
+def solve_scattering_2d_lippmann_schwinger(potential_grid, energy_ev, pixel_size_A, pad_factor=2,
+                                           absorb_frac=0.15, absorb_strength=4.0, gmres_tol=1e-4,
+                                           gmres_restart=70):
+    """(I - G V_scale V) psi = psi_inc by restarted GMRES on the padded grid
+    (:517-602); psi_inc = exp(i k0 y) along axis 1; returns the unpadded psi."""
+    import scipy.sparse.linalg as sla
+    m0, hc = 510998.95000, 12398.4193
+    hbar = HPLANCK / (2 * np.pi)
+    gamma = 1.0 + energy_ev / (M_E * C_LIGHT ** 2 / Q_E)
+    V_scale = -(2.0 * gamma * M_E * Q_E / hbar ** 2) * 1e-20
+    k0 = 2 * np.pi / (hc / np.sqrt(energy_ev * (energy_ev + 2 * m0)))
+    orig = np.shape(potential_grid)
+    padded = [s * pad_factor for s in orig]
+    pad = [((p - o) // 2, (p - o) - (p - o) // 2) for p, o in zip(padded, orig)]
+    Vp = np.pad(np.asarray(potential_grid, dtype=np.float64), pad, mode="constant")
+    Khat, emb = build_lippmann_schwinger_kernel_2d(float(k0), float(pixel_size_A), float(pixel_size_A),
+                                                   padded[0], padded[1])
+
+    def matvec(v):
+        psi = v.reshape(padded)
+        return (psi - apply_convolution(V_scale * Vp * psi, Khat, emb, padded)).ravel()
+
+    y = np.arange(padded[1]) * pixel_size_A
+    y = y - y.mean()
+    b = np.broadcast_to(np.exp(1j * k0 * y), padded).ravel()
+    n = b.size
+    op = sla.LinearOperator((n, n), matvec=matvec, dtype=np.complex128)
+    x, _ = sla.gmres(op, b, rtol=gmres_tol, atol=0.0, restart=gmres_restart)
+    x = x.reshape(padded)
+    return x[pad[0][0]:pad[0][0] + orig[0], pad[1][0]:pad[1][0] + orig[1]]
 
 
 # ---------------------------------------------------------------------------

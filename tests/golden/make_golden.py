@@ -9,6 +9,11 @@ here.  This script installs minimal stand-ins *for this process only*:
   take_along_axis, where, roll, stack, linspace);
 * ``jax.jit``    -> identity (static_argnames accepted and ignored);
 * ``jax.vmap``   -> a Python loop over the mapped axis + np.stack;
+* ``jnp.zeros``  -> NumPy arrays that also offer JAX's functional
+  ``.at[idx].set(v)`` (used by the Lippmann-Schwinger convolution);
+* ``jax.scipy.sparse.linalg.gmres`` -> SciPy's restarted GMRES with the same
+  relative tolerance and restart length (the solve is therefore pinned to
+  within that tolerance, the kernel and the convolution exactly);
 * ``ase.units``  -> ASE's default CODATA-2014 constants;
 * ``abtem.*``    -> empty placeholders (only used by get_abtem_transmit, which
   is not on the path).
@@ -64,9 +69,46 @@ def _install_stubs():
         if not name.startswith("__"):
             setattr(jnp, name, getattr(np, name))
     jnp.fft = np.fft
+
+    class _AtArray(np.ndarray):
+        """ndarray with JAX's functional index update, a.at[idx].set(v)."""
+        @property
+        def at(self):
+            arr = self
+
+            class _Idx:
+                def __getitem__(self, idx):
+                    class _Set:
+                        def set(self, v):
+                            out = np.array(arr)
+                            out[idx] = v
+                            return out.view(_AtArray)
+                    return _Set()
+            return _Idx()
+
+    jnp.zeros = lambda *a, **k: np.zeros(*a, **k).view(_AtArray)
     jax.numpy = jnp
     sys.modules["jax"] = jax
     sys.modules["jax.numpy"] = jnp
+
+    import scipy.sparse.linalg as _sla
+    jsp = types.ModuleType("jax.scipy")
+    jsp_sparse = types.ModuleType("jax.scipy.sparse")
+    jsp_linalg = types.ModuleType("jax.scipy.sparse.linalg")
+
+    def gmres(A, b, x0=None, tol=1e-5, atol=0.0, restart=20, maxiter=None, M=None):
+        b = np.asarray(b)
+        op = _sla.LinearOperator((b.size, b.size), matvec=lambda v: np.asarray(A(v)), dtype=np.complex128)
+        x, info = _sla.gmres(op, b, rtol=tol, atol=atol, restart=restart, maxiter=maxiter)
+        return x, info
+
+    jsp_linalg.gmres = gmres
+    jsp_sparse.linalg = jsp_linalg
+    jsp.sparse = jsp_sparse
+    jax.scipy = jsp
+    sys.modules["jax.scipy"] = jsp
+    sys.modules["jax.scipy.sparse"] = jsp_sparse
+    sys.modules["jax.scipy.sparse.linalg"] = jsp_linalg
 
     abtem = types.ModuleType("abtem")
     ms = types.ModuleType("abtem.multislice")
@@ -222,6 +264,16 @@ def make(ref_root: str, out: str):
     nmap = ref.electron_refractive_index(Vn, E)
     g.update(naive_wave=wave, naive_n=np.asarray(nmap), naive_meta=np.array([ny, nx, ps, dz, E]),
              naive_out=np.asarray(ref.wpm_step(wave, nmap, dz, E, (ps, ps))))
+
+    # --- Lippmann-Schwinger 2D: Green's function kernel, one convolution, a solve --
+    k0_ls, h_ls, n_ls = 2 * np.pi / 0.4, 0.05, 24
+    Khat, emb = ref.build_lippmann_schwinger_kernel_2d(k0_ls, h_ls, h_ls, n_ls, n_ls)
+    src = rng.normal(size=(n_ls, n_ls)) + 1j * rng.normal(size=(n_ls, n_ls))
+    g.update(ls_meta=np.array([k0_ls, h_ls, n_ls]), ls_Khat=np.asarray(Khat), ls_src=src,
+             ls_conv=np.asarray(ref.apply_convolution(src, Khat, emb, (n_ls, n_ls))))
+    Vls = _gauss_stack(rng, 1, 16, 16, 0.1, 3, 20.0, 0.3)[0] / 2.0
+    psi_ls = ref.solve_scattering_2d_lippmann_schwinger(Vls, 200e3, 0.1, gmres_tol=1e-6, gmres_restart=70)
+    g.update(ls_V=Vls, ls_psi=np.asarray(psi_ls), ls_solve_meta=np.array([200e3, 0.1, 1e-6]))
 
     # --- 1D helpers (k0 small enough that the AS kernel has evanescent parts) --
     n1, dx1, dy1, k01 = 64, 0.35, 1.7, 7.0

@@ -115,3 +115,15 @@ def test_1d_helpers(golden):
     psik = np.fft.fft(golden["l1_psi"][0])
     assert O.rel_l2(O.wpm_kernel_1d(psik, 1.3, k0, kx ** 2, dy), golden["l1_wpm1"]) < 1e-13
     assert O.rel_l2(O.wpm_kernel_1d_vmap(psik, golden["l1_nvals"], k0, kx ** 2, dy), golden["l1_wpmv"]) < 1e-13
+
+
+def test_lippmann_schwinger(golden):
+    k0, h, n = golden["ls_meta"]
+    n = int(n)
+    Khat, emb = O.build_lippmann_schwinger_kernel_2d(k0, h, h, n, n)
+    assert emb == (2 * n, 2 * n)
+    assert O.rel_l2(Khat, golden["ls_Khat"]) < 1e-13
+    assert O.rel_l2(O.apply_convolution(golden["ls_src"], Khat, emb, (n, n)), golden["ls_conv"]) < 1e-13
+    E, ps, tol = golden["ls_solve_meta"]
+    psi = O.solve_scattering_2d_lippmann_schwinger(golden["ls_V"], E, ps, gmres_tol=tol)
+    assert O.rel_l2(psi, golden["ls_psi"]) < 1e-10

@@ -7,6 +7,7 @@ from .propagation import *  # noqa: F401,F403
 from .propagation import Plan, get_plan  # noqa: F401
 from .lines import *  # noqa: F401,F403
 from .potentials import gaussian_potential  # noqa: F401
+from .lippmann_schwinger import *  # noqa: F401,F403
 from . import physics, synthetic  # noqa: F401
 
 __version__ = "0.1.0"
