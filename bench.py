@@ -57,6 +57,10 @@ def parse():
                     help="gradient case for ncu captures: the 512^2 x 64-slice inverse problem on a 4x4 probe "
                          "raster (16 probes), checkpoint every 8, two forward + backward steps through the "
                          "persistent scheduler")
+    ap.add_argument("--table", action="store_true",
+                    help="per-configuration table (C1 Fresnel 256^2, C2 AS 1024^2, C3 WPM 512^2; one probe): B200 "
+                         "time, CPU FP64/FP32 restatement on a bounded sample, error vs the FP64 oracle at full "
+                         "size, roofline fraction; prints one JSON object")
     ap.add_argument("--mode", default="persistent", choices=["persistent", "batched", "graph"],
                     help="batched execution mode timed as the headline")
     ap.add_argument("--profile-case", action="store_true",
@@ -186,6 +190,9 @@ def main():
     args = parse()
     if args.profile_grad:
         profile_grad()
+        return
+    if args.table:
+        baseline_table()
         return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
@@ -367,6 +374,80 @@ def _plain(classes, args):
     return {"plain": {"value": rate, "unit": "slice-steps/s", "sample": "16 probes per class, one probe per launch"},
             "per_class_slice_steps_per_s": {f"{c.ny}x{c.nx}": {"batched": 1 / b, "plain": 1 / p}
                                             for c, b, p in zip(classes, bper, per)}}
+
+
+def baseline_table():
+    """One row per single-probe configuration: device time through the public
+    API (inputs resident, no wavefront stack), error vs the FP64 oracle on
+    the full configuration, the oracle in FP64 and FP32 on the host cores
+    (best of 3 after a warm-up, reduced slice counts, per slice-step), and the
+    roofline fraction at 20 B per pixel-slice-step."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    from oracle import propagation_oracle as O
+    S = wap.synthetic
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cores = os.cpu_count() or 1
+    O.set_workers(cores)
+    peak, src = _peak_hbm()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timeit(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    def cpu_rate(fn, n_slices):
+        fn()
+        best = min(_wall(fn) for _ in range(3))
+        return n_slices / best
+
+    rows = {}
+    for name, w, kind, cpu_slices in (("C1_fresnel_256_N20", S.plain_fresnel(0), "fresnel", 20),
+                                      ("C2_as_1024_N100", S.angular_spectrum_diamond(0), "as", 10),
+                                      ("C3_wpm_512_N200_K16", S.wpm_fcc(0), "wpm", 4)):
+        V = torch.as_tensor(w.potential[0], device=dev)
+        pr = torch.as_tensor(w.probe, device=dev)
+        Vh = w.potential[0].astype(np.float64)
+        if kind == "wpm":
+            gpu = lambda: wap.simulate_wpm(V, pr, w.dz, w.energy, (w.ps, w.ps), w.n_bins, w.power_spacing,
+                                           return_wavefronts=False)
+            ref = O.simulate_wpm(Vh, w.probe, w.dz, w.energy, (w.ps, w.ps), w.n_bins, w.power_spacing,
+                                 mode="fp64", return_wavefronts=False)
+            cpu = {m: cpu_rate(lambda m=m: O.simulate_wpm(Vh[:cpu_slices], w.probe, w.dz, w.energy, (w.ps, w.ps),
+                                                         w.n_bins, w.power_spacing, mode=m, return_wavefronts=False),
+                               cpu_slices) for m in ("fp64", "fp32")}
+        else:
+            tf = O.fresnel_propagation_kernel if kind == "fresnel" else O.angular_spectrum_propagation_kernel
+            H = (wap.fresnel_propagation_kernel if kind == "fresnel" else wap.angular_spectrum_propagation_kernel)(
+                w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+            Ho = tf(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+            gpu = lambda: wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
+            ref = O.simulate_fresnel_as(Vh, w.probe, Ho, w.dz, w.energy, mode="fp64", return_wavefronts=False)
+            cpu = {m: cpu_rate(lambda m=m: O.simulate_fresnel_as(Vh[:cpu_slices], w.probe, Ho, w.dz, w.energy,
+                                                                mode=m, return_wavefronts=False), cpu_slices)
+                   for m in ("fp64", "fp32")}
+        ms = timeit(gpu, 5 if kind != "wpm" else 2)
+        ex, dp, _ = gpu()
+        rows[name] = {
+            "gpu_ms_per_call": ms, "gpu_slice_steps_per_s": w.n_slices / (ms / 1e3),
+            "roofline_frac": 20.0 * w.ny * w.nx * w.n_slices / (ms / 1e3) / 1e9 / peak,
+            "err_vs_fp64_exit": float(O.rel_l2(ex.cpu().numpy(), ref[0])),
+            "err_vs_fp64_dp": float(O.rel_l2(dp.cpu().numpy(), ref[1])),
+            "cpu_fp64_slice_steps_per_s": cpu["fp64"], "cpu_fp32_slice_steps_per_s": cpu["fp32"],
+            "cpu_sample_slices": cpu_slices, "cores": cores}
+    print(json.dumps({"table": rows, "peak_gbs": peak, "peak_source": src}), flush=True)
+
+
+def _wall(fn):
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
 
 
 def _configs():
