@@ -128,7 +128,8 @@ static cudaError_t launch_wpm_col_t(const WpmColArgs& a, int nb, int w, cudaStre
   cudaError_t err = prep_smem(wpm_col_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
   count_launch();
-  wpm_col_kernel<N, E><<<dim3(a.nx / w, nb), w * FFTPlan<N, E>::T, smem, st>>>(a);
+  const int groups = a.dp_mode ? 1 : (a.K + a.kpg - 1) / a.kpg;
+  wpm_col_kernel<N, E><<<dim3(a.nx / w, nb, groups), w * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -139,8 +140,33 @@ static cudaError_t launch_wpm_row_t(const WpmRowArgs& a, int nb, int rows, cudaS
   cudaError_t err = prep_smem(wpm_row_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
   count_launch();
-  wpm_row_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
+  const int groups = a.blend ? (a.K - 1 + a.kpg - 1) / a.kpg : 1;
+  wpm_row_kernel<N, E><<<dim3(a.ny / rows, nb, groups), rows * FFTPlan<N, E>::T, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+// resident CTAs per SM of the WPM kernels at a launch shape (0 on error)
+template <int N, int E>
+static int occ_wpm_col_t(int w, int K) {
+  const size_t smem = col_smem_bytes<N, E>(w, K * (int)sizeof(float));
+  int n = 0;
+  if (prep_smem(wpm_col_kernel<N, E>, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wpm_col_kernel<N, E>, w * FFTPlan<N, E>::T, smem) !=
+      cudaSuccess)
+    return 0;
+  return n;
+}
+
+template <int N, int E>
+static int occ_wpm_row_t(int rows, int K) {
+  const int extra = K * (int)sizeof(float) + ((K + 31) / 32) * (int)sizeof(unsigned);
+  const size_t smem = row_smem_bytes<N, E>(rows, extra);
+  int n = 0;
+  if (prep_smem(wpm_row_kernel<N, E>, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wpm_row_kernel<N, E>, rows * FFTPlan<N, E>::T, smem) !=
+      cudaSuccess)
+    return 0;
+  return n;
 }
 
 #define WAP_SIZE_CASES(M, E) \
@@ -159,11 +185,24 @@ static cudaError_t launch_wpm_row_t(const WpmRowArgs& a, int nb, int rows, cudaS
 #define WAP_CASE_col(N, E) case E * 100000 + N: return launch_col_t<N, E>(a, nb, k, st);
 #define WAP_CASE_wcol(N, E) case E * 100000 + N: return launch_wpm_col_t<N, E>(a, nb, k, st);
 #define WAP_CASE_wrow(N, E) case E * 100000 + N: return launch_wpm_row_t<N, E>(a, nb, k, st);
+#define WAP_CASE_wcolocc(N, E) case E * 100000 + N: return occ_wpm_col_t<N, E>(k, K);
+#define WAP_CASE_wrowocc(N, E) case E * 100000 + N: return occ_wpm_row_t<N, E>(k, K);
+
+#define WAP_DISPATCH_INT(FN, n, e)                                      \
+  do {                                                                  \
+    switch ((e) * 100000 + (n)) {                                       \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 8)                                  \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 16)                                 \
+      default: return 0;                                                \
+    }                                                                   \
+  } while (0)
 
 cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(row, n, e); }
 cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(col, n, e); }
 cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wcol, n, e); }
 cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wrow, n, e); }
+int wpm_col_occupancy(int n, int e, int k, int K) { WAP_DISPATCH_INT(wcolocc, n, e); }
+int wpm_row_occupancy(int n, int e, int k, int K) { WAP_DISPATCH_INT(wrowocc, n, e); }
 
 bool size_supported(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0; }
 
@@ -293,6 +332,7 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
     const size_t plane = (size_t)ny * nx;
     cudaError_t err = cudaMalloc(&p->fields, (size_t)max_batch * n_bins * plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->dpbuf, (size_t)max_batch * plane * sizeof(float2));
+    if (err == cudaSuccess) err = cudaMalloc(&p->blend, (size_t)max_batch * plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->hvac, plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->hvac_lo, plane * sizeof(float2));
     if (err == cudaSuccess) err = cudaMalloc(&p->ky2, ny * sizeof(float));
@@ -313,6 +353,7 @@ int wap_plan_destroy(wap_plan* p) {
   cudaFree(p->tw_col);
   cudaFree(p->fields);
   cudaFree(p->dpbuf);
+  cudaFree(p->blend);
   cudaFree(p->hvac);
   cudaFree(p->hvac_lo);
   cudaFree(p->ky2);

@@ -29,6 +29,7 @@ struct wap_plan {
   // WPM workspace
   float2* fields = nullptr;                 // (max_batch, n_bins, ny, nx)
   float2* dpbuf = nullptr;                  // (max_batch, ny, nx)
+  float2* blend = nullptr;                  // (max_batch, ny, nx) WPM bin-split blend
   float2* hvac = nullptr;                   // (ny, nx) hi part
   float2* hvac_lo = nullptr;                // (ny, nx) lo part
   float* ky2 = nullptr;
@@ -68,6 +69,9 @@ cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream
 cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st);
 cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cudaStream_t st);
 cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st);
+// resident CTAs per SM of the WPM column (k = columns per CTA) and row (k = rows per CTA) kernels
+int wpm_col_occupancy(int n, int e, int k, int K);
+int wpm_row_occupancy(int n, int e, int k, int K);
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
 RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
 int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st);

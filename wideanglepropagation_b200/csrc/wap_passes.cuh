@@ -486,6 +486,7 @@ struct WpmColArgs {
   float* dp;                 // dp mode: |fft2|^2 (fftshifted, detector window), no fields
   Detector det;
   int ny, nx, K, slice, n_slices, probe0, dp_mode;
+  int kpg;                   // bins per CTA group (blockIdx.z): bins [z kpg, min(z kpg + kpg, K))
   float k02;                 // k0^2
   float dz;
 };
@@ -548,7 +549,8 @@ wpm_col_kernel(const WpmColArgs a) {
   for (int e = 0; e < E; ++e) sq0[e] = sqrtf(fabsf(q0[e]));
 
   float2* ftile = a.fields + (long long)b * a.K * plane + (long long)blockIdx.x * W;
-  for (int k = 0; k < a.K; ++k) {
+  const int kb = blockIdx.z * a.kpg, ke = min(kb + a.kpg, a.K);
+  for (int k = kb; k < ke; ++k) {
     const float dk = srefs[k];
     const float ak = a.k02 * dk * (2.0f + dk);   // n_k^2 k0^2 - k0^2
     float2 u[E];
@@ -606,6 +608,12 @@ struct WpmRowArgs {
   int ny, nx, K, slice, n_slices, probe0, last;
   float scale;               // 1/(ny nx)
   float ri_a, ri_inv_den;
+  // Bin-split mode (blend != null): CTA group z owns the pixels whose left
+  // bin lies in [z kpg, min(z kpg + kpg, K - 1)), transforms the bins it needs
+  // (its own and the next group's first), and stores the owned pixels' blend
+  // into `blend`; a row pass then applies the forward row FFT.
+  float2* blend;
+  int kpg;
 };
 
 template <int NX, int E>
@@ -637,6 +645,9 @@ wpm_row_kernel(const WpmRowArgs a) {
   const int K = a.K;
 
   // bracketing bins and smoothstep weights (propagation.py:239-249)
+  const bool split = a.blend != nullptr;
+  const int kb = split ? blockIdx.z * a.kpg : 0;           // owned left bins [kb, kl)
+  const int kl = split ? min(kb + a.kpg, K - 1) : K - 1;
   int il[E];
   float wr[E];
   const float* vrow = a.V + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
@@ -656,8 +667,10 @@ wpm_row_kernel(const WpmRowArgs a) {
     w = fminf(fmaxf(w, 0.0f), 1.0f);
     wr[e] = w * w * (3.0f - 2.0f * w);
     il[e] = ir - 1;
-    atomicOr(used + ((ir - 1) >> 5), 1u << ((ir - 1) & 31));
-    atomicOr(used + (ir >> 5), 1u << (ir & 31));
+    if (ir - 1 >= kb && ir - 1 < kl) {
+      atomicOr(used + ((ir - 1) >> 5), 1u << ((ir - 1) & 31));
+      atomicOr(used + (ir >> 5), 1u << (ir & 31));
+    }
   }
   __syncthreads();
 
@@ -665,7 +678,7 @@ wpm_row_kernel(const WpmRowArgs a) {
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
   const float2* frow = a.fields + (long long)b * K * plane + (long long)row * NX;
-  for (int k = 0; k < K; ++k) {
+  for (int k = kb; k <= kl; ++k) {
     if (!(used[k >> 5] & (1u << (k & 31)))) continue;   // CTA-uniform
     float2 u[E];
     const float2* fk = frow + (long long)k * plane;
@@ -680,6 +693,14 @@ wpm_row_kernel(const WpmRowArgs a) {
   }
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = cscale(acc[e], a.scale);
+
+  if (split) {
+    float2* brow = a.blend + (long long)b * plane + (long long)row * NX;
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (il[e] >= kb && il[e] < kl) __stcg(brow + t + T * e, acc[e]);
+    return;
+  }
 
   if (a.snap) {
     float2* sp = a.snap + (long long)b * a.snap_bstride + (long long)row * NX;

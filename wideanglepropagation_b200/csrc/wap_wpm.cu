@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 
 #include "wap_internal.h"
 #include "wap_passes.cuh"
@@ -144,10 +145,46 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
   w.snap_bstride = (long long)n_slices * plane;
   const int rows = rows_per_cta(p->nx, p->row_e, p->ny);
 
+  // Few probes leave most SMs idle (a 512^2 probe is 128 column and 128 row
+  // CTAs): then the K bins are split across CTA groups - each column CTA
+  // redoes the column FFT for its share of the bins, each row CTA blends the
+  // pixels whose left bin is in its share, and a row pass applies the row FFT.
+  // The group count minimises (waves of resident CTAs) x (transforms per CTA).
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+  const int col_slots = std::max(1, wpm_col_occupancy(p->ny, p->col_e, p->col_w, K)) * sms;
+  const int row_slots = std::max(1, wpm_row_occupancy(p->nx, p->row_e, rows, K)) * sms;
+  // Bins per group (the launched group count is ceil(units / per)).  Column
+  // CTA: 1 + per transforms; row CTA: K transforms unsplit, else per + 1 and
+  // the row pass that follows (counted as one more).
+  auto best_per = [&](long long ctas0, int slots, int units, bool col) {
+    int best = units;
+    double best_cost = 1e300;
+    for (int per = units; per >= 1; --per) {
+      const long long g = (units + per - 1) / per;
+      const double waves = std::ceil((double)(ctas0 * g) / slots);
+      const double work = col ? 1.0 + per : (g == 1 ? (double)K : per + 2.0);
+      if (waves * work < best_cost) {
+        best_cost = waves * work;
+        best = per;
+      }
+    }
+    return best;
+  };
+
   for (int b0 = 0; b0 < n_probes; b0 += 65535) {
     const int nb = std::min(65535, n_probes - b0);
     c.probe0 = b0;
     w.probe0 = b0;
+    c.kpg = best_per((long long)(p->nx / p->col_w) * nb, col_slots, K, true);
+    w.kpg = best_per((long long)(p->ny / rows) * nb, row_slots, K - 1, false);
+    const int gr = (K - 1 + w.kpg - 1) / w.kpg;
+    w.blend = gr > 1 ? p->blend : nullptr;
+    RowArgs fin = base_row_args(p, ph, V, n_slices, draw);   // the row FFT after a bin-split blend
+    fin.src = p->blend;
+    fin.src_bstride = plane;
+    fin.shifts = nullptr;
+    fin.flags = ROW_LOAD_SRC | ROW_FFT;
     for (int s = 0; s < n_slices; ++s) {
       c.slice = s;
       c.dp_mode = 0;
@@ -162,6 +199,21 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
       if ((e = launch_wpm_row(p->nx, p->row_e, w, nb, rows, st)) != cudaSuccess) return cuda_fail(e, "wpm row pass");
       // K fields in, potential, wave out (+ dp buffer on the last slice, + snapshot)
       prof_end(tok, st, (8.0 * K + 4.0 + 8.0 + (w.last ? 8.0 : 0.0) + (w.snap ? 8.0 : 0.0)) * plane * nb);
+      if (w.blend) {
+        // row FFT of the blended wave; the spatial wave is this slice's snapshot
+        // (at the last slice: the exit wave, the transform going to the dp buffer)
+        fin.probe0 = b0;
+        fin.psi = w.last ? p->dpbuf : reinterpret_cast<float2*>(exit);
+        fin.psi_bstride = plane;
+        fin.snap = w.last ? reinterpret_cast<float2*>(exit) : w.snap;
+        fin.snap_bstride = w.last ? plane : (long long)n_slices * plane;
+        if ((e = launch_row(p->nx, p->row_e, fin, nb, rows, st)) != cudaSuccess) return cuda_fail(e, "wpm row FFT");
+        if (w.last && w.snap &&
+            (e = cudaMemcpy2DAsync(w.snap + (long long)b0 * n_slices * plane, (size_t)n_slices * plane * sizeof(float2),
+                                   reinterpret_cast<float2*>(exit) + (long long)b0 * plane, plane * sizeof(float2),
+                                   plane * sizeof(float2), nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+          return cuda_fail(e, "wpm last snapshot");
+      }
     }
     if (dp) {
       WpmColArgs d = c;
