@@ -27,6 +27,15 @@ def _key(ny, nx, op, n_bins, batch_class="any") -> str:
     return f"{_gpu_name()}|{ny}x{nx}|op{op}|K{n_bins}|{batch_class}"
 
 
+SINGLE_MAX = 2   # calls with at most this many probes use the "single" launch shapes
+
+
+def batch_class(batch: int) -> str:
+    """'single' for one or two probes (few CTAs per pass: the shape must spread
+    them over the SMs), 'any' otherwise."""
+    return "single" if batch <= SINGLE_MAX else "any"
+
+
 def _load() -> dict:
     global _cache
     if _cache is None:
@@ -38,17 +47,19 @@ def _load() -> dict:
     return _cache
 
 
-def lookup(ny, nx, op, n_bins=0):
-    """Cached (row_e, col_e, col_w) for this GPU and grid, or None."""
+def lookup(ny, nx, op, n_bins=0, cls="any"):
+    """Cached (row_e, col_e, col_w) for this GPU, grid and batch class (falling
+    back to the 'any' entry), or None."""
     with _lock:
-        v = _load().get(_key(ny, nx, op, n_bins))
+        c = _load()
+        v = c.get(_key(ny, nx, op, n_bins, cls)) or c.get(_key(ny, nx, op, n_bins))
     return tuple(v) if v else None
 
 
-def store(ny, nx, op, n_bins, cfg) -> None:
+def store(ny, nx, op, n_bins, cfg, cls="any") -> None:
     with _lock:
         c = _load()
-        c[_key(ny, nx, op, n_bins)] = list(cfg)
+        c[_key(ny, nx, op, n_bins, cls)] = list(cfg)
         tmp = CACHE_PATH + ".tmp"
         with open(tmp, "w") as f:
             json.dump(c, f, indent=1, sort_keys=True)
@@ -122,7 +133,7 @@ def tune(ny: int, nx: int, op: int = 0, n_bins: int = 0, batch: int | None = Non
             print(f"  {ny}x{nx} op{op} {cfg}: {times[cfg]:.3f} ms", flush=True)
     best = min(times, key=times.get)
     plan.set_config(*best) if best else plan.set_config(*old)
-    store(ny, nx, op, n_bins, best)
+    store(ny, nx, op, n_bins, best, batch_class(batch))
     return best, times
 
 
@@ -131,12 +142,14 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="autotune the multislice launch shapes on this GPU")
     ap.add_argument("--grids", default="256,512,1024", help="comma-separated square grid sizes")
     ap.add_argument("--wpm-bins", default="16", help="comma-separated WPM bin counts to tune (empty: none)")
+    ap.add_argument("--single", action="store_true", help="tune the single-probe shapes (batch 1) instead")
     args = ap.parse_args(argv)
+    b = 1 if args.single else None
     for n in [int(v) for v in args.grids.split(",") if v]:
-        best, _ = tune(n, n, 0, 0, verbose=True)
+        best, _ = tune(n, n, 0, 0, batch=b, verbose=True)
         print(f"{n}x{n} fresnel/as best {best}", flush=True)
         for k in [int(v) for v in args.wpm_bins.split(",") if v]:
-            best, _ = tune(n, n, 1, k, verbose=True)
+            best, _ = tune(n, n, 1, k, batch=b, verbose=True)
             print(f"{n}x{n} wpm K={k} best {best}", flush=True)
     print(f"cache: {CACHE_PATH}")
 

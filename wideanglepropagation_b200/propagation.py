@@ -148,18 +148,21 @@ _plans_lock = threading.Lock()
 
 
 def get_plan(ny: int, nx: int, batch: int, op: int, n_bins: int = 0) -> Plan:
-    """Cached plan for (device, grid, op, bins) holding at least ``batch`` probes."""
+    """Cached plan for (device, grid, op, bins, batch class) holding at least
+    ``batch`` probes; one- and two-probe calls get their own plan with the
+    launch shapes tuned for them."""
+    from . import autotune
     dev = torch.cuda.current_device()
-    key = (dev, ny, nx, op, n_bins)
+    cls = autotune.batch_class(batch)
+    key = (dev, ny, nx, op, n_bins, cls)
     with _plans_lock:
         p = _plans.get(key)
         if p is None or p.max_batch < batch:
             if p is not None:
                 p.close()
-            cap = batch if op == _lib.WAP_OP_WPM else max(batch, 64)
+            cap = batch if (op == _lib.WAP_OP_WPM or cls == "single") else max(batch, 64)
             p = Plan(ny, nx, cap, op, n_bins)
-            from . import autotune
-            cfg = autotune.lookup(ny, nx, op, n_bins)
+            cfg = autotune.lookup(ny, nx, op, n_bins, cls)
             if cfg is not None:
                 p.set_config(*cfg)
             _plans[key] = p
