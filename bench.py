@@ -57,6 +57,8 @@ def parse():
                     help="gradient case for ncu captures: the 512^2 x 64-slice inverse problem on a 4x4 probe "
                          "raster (16 probes), checkpoint every 8, two forward + backward steps through the "
                          "persistent scheduler")
+    ap.add_argument("--profile-wpm", action="store_true",
+                    help="WPM case for ncu captures: C3 (512^2, K=16, plane wave) at 3 slices, two calls")
     ap.add_argument("--table", action="store_true",
                     help="per-configuration table (C1 Fresnel 256^2, C2 AS 1024^2, C3 WPM 512^2; one probe): B200 "
                          "time, CPU FP64/FP32 restatement on a bounded sample, error vs the FP64 oracle at full "
@@ -193,6 +195,9 @@ def main():
         return
     if args.table:
         baseline_table()
+        return
+    if args.profile_wpm:
+        profile_wpm()
         return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
@@ -374,6 +379,19 @@ def _plain(classes, args):
     return {"plain": {"value": rate, "unit": "slice-steps/s", "sample": "16 probes per class, one probe per launch"},
             "per_class_slice_steps_per_s": {f"{c.ny}x{c.nx}": {"batched": 1 / b, "plain": 1 / p}
                                             for c, b, p in zip(classes, bper, per)}}
+
+
+def profile_wpm():
+    import torch
+    import wideanglepropagation_b200 as wap
+    w = wap.synthetic.wpm_fcc(0, n_slices=3)
+    dev = torch.device("cuda", 0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    for _ in range(2):
+        wap.simulate_wpm(V, pr, w.dz, w.energy, (w.ps, w.ps), w.n_bins, w.power_spacing, return_wavefronts=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_wpm": "ok"}))
 
 
 def baseline_table():
