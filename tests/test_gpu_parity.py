@@ -240,3 +240,29 @@ def test_unsupported_size_raises(wap):
     with pytest.raises(ValueError, match="unsupported grid"):
         wap.simulate_fresnel_as(np.zeros((1, 100, 100), np.float32), np.ones((100, 100), np.complex64),
                                 np.ones((100, 100), np.complex64), 1.0, 200e3)
+
+
+def test_pinned_host_inputs_upload_on_a_side_stream(wap):
+    """Pinned host arrays (uploaded on a side stream that the caller's stream
+    waits for) give the same result as device arrays, also when the upload is
+    queued behind a long call on the caller's stream."""
+    import wideanglepropagation_b200.synthetic as S
+    ws = S.batched_scan(0, small=True)
+    w = ws[1]
+    H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    dev = torch.device("cuda")
+    Vd, pd = torch.as_tensor(w.potential, device=dev), torch.as_tensor(w.probe, device=dev)
+    qd, dd = torch.as_tensor(w.positions, device=dev), torch.as_tensor(w.draw_of_probe, device=dev)
+    ref_ex, ref_dp, _ = wap.simulate_fresnel_as(Vd, pd, H, w.dz, w.energy, positions=qd, draw=dd,
+                                                return_wavefronts=False)
+    Vh = torch.from_numpy(w.potential).pin_memory()
+    big = torch.zeros((16, 512, 512), dtype=torch.float32, device=dev)
+    Hb = wap.fresnel_propagation_kernel(512, 512, (0.05, 0.05), 2.0, 300e3)
+    for _ in range(2):
+        wap.simulate_fresnel_as(big, torch.ones((512, 512), dtype=torch.complex64, device=dev), Hb, 2.0, 300e3,
+                                return_wavefronts=False)   # keeps the caller's stream busy
+        ex, dp, _ = wap.simulate_fresnel_as(Vh, torch.from_numpy(w.probe).pin_memory(), H, w.dz, w.energy,
+                                            positions=torch.from_numpy(w.positions).pin_memory(),
+                                            draw=torch.from_numpy(w.draw_of_probe).pin_memory(),
+                                            return_wavefronts=False)
+        assert torch.equal(ex, ref_ex) and torch.equal(dp, ref_dp)

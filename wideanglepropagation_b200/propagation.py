@@ -59,11 +59,36 @@ def _device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
+_copy_streams: dict = {}
+
+
+def _copy_stream(device) -> torch.cuda.Stream:
+    key = torch.device(device).index
+    s = _copy_streams.get(key)
+    if s is None:
+        s = _copy_streams[key] = torch.cuda.Stream(device=device)
+    return s
+
+
 def _to(x, dtype, device) -> torch.Tensor:
     if not isinstance(x, torch.Tensor):
         x = torch.as_tensor(np.asarray(x))
     if x.is_complex() and not dtype.is_complex:
         raise ValueError("expected a real array, got a complex one")
+    if (x.device.type == "cpu" and x.dtype == dtype and x.is_contiguous() and x.numel() > 0
+            and torch.device(device).type == "cuda" and x.is_pinned()):
+        # Pinned host input: copy on a side stream so the upload overlaps the
+        # kernels already queued on the caller's stream; the caller's stream
+        # waits for the copy before it uses the data.  (As with any
+        # non-blocking copy, the host buffer must not change until then.)
+        cur = torch.cuda.current_stream(device)
+        cs = _copy_stream(device)
+        with torch.cuda.stream(cs):
+            y = torch.empty(x.shape, dtype=dtype, device=device)
+            y.copy_(x, non_blocking=True)
+        cur.wait_stream(cs)
+        y.record_stream(cur)
+        return y
     return x.to(device=device, dtype=dtype).contiguous()
 
 
