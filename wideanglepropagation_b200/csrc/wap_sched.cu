@@ -124,7 +124,7 @@ struct SchedClass {
   float2* ckpt;                 // (B, nck, n, n) checkpoints
   int ckpt_n, seg_n;            // slots per probe
   int ckpt_k;                   // gradient scans: checkpoint every ckpt_k slices (0: none)
-  int seg_first;                // first slice of the last segment (kept by the forward)
+  int seg_first;                // first slice of the trailing segments the forward keeps
   const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp (full grid)
   float* grad;                  // (draws, N, n, n) probe sums of Re(conj(lambda_a) i a_s)
   float ri_a, ri_inv_den, kphase, e_plus_e0;
@@ -947,15 +947,24 @@ static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map
   return WAP_OK;
 }
 
+// Trailing checkpoint segments whose waves the forward keeps, so that the
+// backward recomputes none of them: memory stays O(sqrt N) - checkpoints every
+// k slices plus 2k waves - and one segment's recompute (2k - 1 passes) drops.
+constexpr int kKeptSegments = 2;
+
+static int kept_first_slice(int n_slices, int k) {
+  const int nck = (n_slices + k - 1) / k;
+  return (nck - std::min(kKeptSegments, nck)) * k;
+}
+
 // Forward chain of one class: steps 0..2N (rows even, columns odd).  With
 // ckpt_every > 0 the rows also store checkpoints (every k-th slice) and the
-// waves of the last k-slice segment after its first slice (whose wave is its
-// checkpoint).
+// waves of the kept trailing segments after their first slice (whose wave is
+// a checkpoint).
 static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, std::vector<Step>& out) {
   const int N = n_slices;
   const int k = ckpt_every;
-  const int nck = k > 0 ? (N + k - 1) / k : 0;
-  const int last0 = k > 0 ? (nck - 1) * k : N;
+  const int last0 = k > 0 ? kept_first_slice(N, k) : N;
   int prefix = 0;
   for (int p = 0; p <= 2 * N; ++p) {
     Step st{};
@@ -979,12 +988,15 @@ static void forward_steps(const SchedClass& sc, int n_slices, int ckpt_every, st
 }
 
 // Backward chain: seed, then per segment (last first) recompute + adjoint.
-// The recompute starts from the segment's checkpoint and keeps the waves
-// entering slices s0+1 .. s1-1; the adjoint row of slice s0 reads the
-// checkpoint itself (one-slice segments need no recompute at all).
+// The kept trailing segments need no recompute: their adjoint rows read the
+// waves the forward stored (slot s - first kept slice).  Earlier segments are
+// recomputed from their checkpoint, keeping the waves entering slices
+// s0+1 .. s1-1; the adjoint row of slice s0 reads the checkpoint itself
+// (one-slice segments need no recompute at all).
 static void backward_steps(const SchedClass& sc, int n_slices, int k, std::vector<Step>& out) {
   const int N = n_slices;
   const int nck = (N + k - 1) / k;
+  const int kept0 = kept_first_slice(N, k);
   int prefix = 0;
   auto push = [&](int type, int slice, int seg0, int ckpt_slot, int seg_slot) {
     Step st{type, slice, seg0, ckpt_slot, seg_slot, prefix};
@@ -995,7 +1007,16 @@ static void backward_steps(const SchedClass& sc, int n_slices, int k, std::vecto
   push(ST_SEED_COL, N - 1, 0, -1, -1);
   for (int j = nck - 1; j >= 0; --j) {
     const int s0 = j * k, s1 = std::min(s0 + k, N);
-    if (j != nck - 1 && s1 - s0 > 1) {
+    if (s0 >= kept0) {
+      for (int s = s1 - 1; s >= s0; --s) {
+        const int type = s == 0 ? ST_ADJ_ROW0 : ST_ADJ_ROW;
+        if (s == kept0) push(type, s, s0, j, -1);   // the first kept slice: checkpoint j
+        else push(type, s, s0, -1, s - kept0);
+        if (s > 0) push(ST_ADJ_COL, s, s0, -1, -1);
+      }
+      continue;
+    }
+    if (s1 - s0 > 1) {
       push(ST_REC_ROW0, s0, s0, j, -1);
       push(ST_REC_COL, s0, s0, -1, -1);
       for (int s = s0 + 1; s < s1 - 1; ++s) {
@@ -1199,11 +1220,12 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     if (s->grad) {
       const int k = ckpt_every;
       sc.ckpt_n = (c.n_slices + k - 1) / k;
-      sc.seg_n = k;
+      sc.seg_first = kept_first_slice(c.n_slices, k);
+      sc.seg_n = std::max(k, c.n_slices - sc.seg_first);   // kept waves, or one recomputed segment
       sc.ckpt_k = k;
-      sc.seg_first = (sc.ckpt_n - 1) * k;
       const size_t plane = (size_t)n * n, B = (size_t)c.n_probes;
-      const size_t sizes[4] = {B * plane * 8, B * plane * 8, B * k * plane * 8, B * sc.ckpt_n * plane * 8};
+      const size_t sizes[4] = {B * plane * 8, B * plane * 8, B * (size_t)sc.seg_n * plane * 8,
+                               B * sc.ckpt_n * plane * 8};
       float2** dsts[4] = {&sc.lam, &sc.work, &sc.seg, &sc.ckpt};
       for (int i = 0; i < 4; ++i) {
         void* p = nullptr;
