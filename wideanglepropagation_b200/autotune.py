@@ -1,10 +1,14 @@
-"""Launch-shape autotuner for the multislice passes.
+"""Launch-shape autotuner for the multislice passes and the persistent scheduler.
 
-Candidates per grid: elements per thread of the row pass (``row_e``), of the
-column pass (``col_e``) and columns per column-pass CTA (``col_w``).  Each is
-timed on the device with CUDA events over a short synthetic multislice; the
-winner is cached in ``autotune_cache.json`` keyed by GPU name, grid, op and
-bin count, and applied to every plan created afterwards.
+Per-pass kernels — candidates per grid: elements per thread of the row pass
+(``row_e``), of the column pass (``col_e``) and columns per column-pass CTA
+(``col_w``), for batched calls and for one- or two-probe calls.  Persistent
+scheduler — the probe-group size (probes advanced together through every pass:
+enough tiles per pass to keep the resident CTAs busy, few enough that the
+group's waves stay in L2).  Each candidate is timed on the device with CUDA
+events over a short synthetic multislice; the winner is cached in
+``autotune_cache.json`` keyed by GPU name, grid, op, bin count and batch class,
+and applied to every plan or scan created afterwards.
 """
 from __future__ import annotations
 
@@ -137,13 +141,83 @@ def tune(ny: int, nx: int, op: int = 0, n_bins: int = 0, batch: int | None = Non
     return best, times
 
 
+def default_scan_group(n: int) -> int:
+    """The scheduler's built-in probe-group size: 4 x the resident CTAs (3 per
+    SM) in tiles, a tile being 4096 pixels (16 elements x 256 threads)."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    row_tiles = max(1, n * n // 4096)
+    return max(1, -(-4 * 3 * sms // row_tiles))
+
+
+def lookup_scan(n: int) -> int:
+    """Cached probe-group size of the persistent scheduler for n x n grids (0: built-in)."""
+    with _lock:
+        v = _load().get(_key(n, n, "scan", 0))
+    return int(v[0]) if v else 0
+
+
+def tune_scan(n: int, n_slices: int = 8, verbose: bool = False):
+    """Time the persistent scheduler on a synthetic n x n scan at probe-group
+    sizes around the built-in one; cache and return the fastest."""
+    import numpy as np
+    import torch
+    from .scan import BatchedScan, DeviceClass
+    from .propagation import transfer_pair
+    g0 = default_scan_group(n)
+    cands = sorted({max(1, g0 // 4), max(1, g0 // 2), max(1, (3 * g0) // 4), g0, (3 * g0) // 2, 2 * g0})
+    B = 8 * g0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gen = torch.Generator(device=dev).manual_seed(0)
+    V = torch.rand((1, n_slices, n, n), generator=gen, device=dev) * 30
+    probe = torch.ones((n, n), dtype=torch.complex64, device=dev)
+    pos = torch.randint(0, n, (B, 2), generator=gen, device=dev, dtype=torch.int32)
+    H, H_lo = transfer_pair("as", n, n, (0.05, 0.05), 2.0, 300e3)
+    cls = DeviceClass(n, n, n_slices, 1, B, 2.0, 300e3, V, probe, pos, torch.zeros(B, dtype=torch.int32, device=dev),
+                      H, H_lo, torch.empty((B, n, n), dtype=torch.complex64, device=dev),
+                      torch.empty((B, n, n), dtype=torch.float32, device=dev))
+    times = {}
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for g in cands:
+        bs = BatchedScan([cls], mode="persistent", groups=[g])
+        bs.step()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(3):
+            s.record()
+            bs.step()
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        times[g] = best
+        if verbose:
+            print(f"  scan {n}x{n} group {g}: {best:.3f} ms", flush=True)
+        del bs
+    best = min(times, key=times.get)
+    with _lock:
+        c = _load()
+        c[_key(n, n, "scan", 0)] = [int(best)]
+        tmp = CACHE_PATH + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(c, f, indent=1, sort_keys=True)
+        os.replace(tmp, CACHE_PATH)
+    return best, times
+
+
 def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser(description="autotune the multislice launch shapes on this GPU")
     ap.add_argument("--grids", default="256,512,1024", help="comma-separated square grid sizes")
     ap.add_argument("--wpm-bins", default="16", help="comma-separated WPM bin counts to tune (empty: none)")
     ap.add_argument("--single", action="store_true", help="tune the single-probe shapes (batch 1) instead")
+    ap.add_argument("--scan", action="store_true", help="tune the persistent scheduler's probe-group size instead")
     args = ap.parse_args(argv)
+    if args.scan:
+        for n in [int(v) for v in args.grids.split(",") if v]:
+            best, _ = tune_scan(n, verbose=True)
+            print(f"{n}x{n} scan group best {best} (built-in {default_scan_group(n)})", flush=True)
+        print(f"cache: {CACHE_PATH}")
+        return
     b = 1 if args.single else None
     for n in [int(v) for v in args.grids.split(",") if v]:
         best, _ = tune(n, n, 0, 0, batch=b, verbose=True)

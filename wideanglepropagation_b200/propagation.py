@@ -362,9 +362,13 @@ def _dp_shape(B, ny, nx, det):
     return (B, det[2], det[3]) if det is not None else (B, ny, nx)
 
 
-def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, group=0):
-    """``wap_scan_class`` for one grid class of device tensors."""
+def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, group=None):
+    """``wap_scan_class`` for one grid class of device tensors; the probe-group
+    size defaults to the autotuned one for the grid (0: the scheduler's own)."""
     D, N, n, _ = V.shape
+    if group is None:
+        from . import autotune
+        group = autotune.lookup_scan(n)
     y0, x0, dny, dnx = det if det is not None else (0, 0, 0, 0)
     return _lib.ScanClass(n, N, D, exit_wave.shape[0], V.data_ptr(), dr.data_ptr() if dr is not None else None,
                           psi.data_ptr(), pos.data_ptr() if pos is not None else None, H.data_ptr(),

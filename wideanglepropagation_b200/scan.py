@@ -94,6 +94,9 @@ class PersistentScan:
     """Owns a ``wap_scan`` (device work queue over all classes)."""
 
     def __init__(self, classes: List[DeviceClass], groups: Optional[List[int]] = None):
+        from . import autotune
+        if groups is None:   # autotuned probe-group sizes (0: the scheduler's own)
+            groups = [autotune.lookup_scan(c.ny) if c.ny == c.nx else 0 for c in classes]
         arr = (_lib.ScanClass * len(classes))()
         for i, c in enumerate(classes):
             if c.ny != c.nx:
@@ -101,7 +104,7 @@ class PersistentScan:
             arr[i] = _lib.ScanClass(c.ny, c.n_slices, c.n_draws, c.n_probes, c.V.data_ptr(), c.draw.data_ptr(),
                                     c.probe.data_ptr(), c.positions.data_ptr(), c.H.data_ptr(),
                                     c.H_lo.data_ptr() if c.H_lo is not None else None, c.dz, c.energy,
-                                    c.exit.data_ptr(), c.dp.data_ptr(), (groups or [0] * len(classes))[i])
+                                    c.exit.data_ptr(), c.dp.data_ptr(), groups[i])
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().wap_scan_create(ctypes.byref(h), len(classes), ctypes.cast(arr, ctypes.c_void_p)))
         self.handle = h
