@@ -291,7 +291,10 @@ def main():
         st = scan.sched.status()
         if st != 0:
             raise RuntimeError(f"persistent scan reported status {st}")
-    if not args.no_extras and rank == 0:
+    # the extras and the CPU baseline belong to the single-GPU line: with N ranks
+    # the others would idle at the next collective while rank 0 runs them
+    extras_on = not args.no_extras and world == 1
+    if extras_on:
         extras.update(_plain(classes, args))
         extras.update(_per_pass(classes, args))
         extras.update(_configs())
@@ -303,14 +306,14 @@ def main():
 
     # --- e2e through the public API from pinned host buffers ------------------
     e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
-    if not args.no_extras:
+    if extras_on:
         # the same with a 50 mrad detector: the crop is fused into the last column pass
         extras["e2e_detector_50mrad"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=50.0)
         # the same from atom lists: the potential is built on the device
         extras["e2e_from_atoms"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, from_atoms=True)
 
     cpu = None
-    if rank == 0 and not args.no_extras:
+    if rank == 0 and extras_on:
         r, cores, desc = cpu_reference_sample(classes_host, scale=4, mode="fp64")
         cpu = {"value": r, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc}
 
