@@ -1,0 +1,82 @@
+"""Edge cases of the drop-in API on the device: empty inputs, the largest
+grid, probe positions that wrap the grid edges on both execution paths,
+odd batch sizes around the scheduler's threshold, and one slice."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def wap():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import wideanglepropagation_b200 as w
+    return w
+
+
+def _setup(n=128, N=3, seed=0):
+    import wideanglepropagation_b200.synthetic as S
+    rng = np.random.default_rng(seed)
+    ps, dz, E = 0.1, 2.0, 200e3
+    V = (S.random_gaussian_stack(rng, N, n, n, ps, 8, 20.0, 0.3) / dz).astype(np.float32)
+    probe = S.aperture_probe(n, n, ps, E, 20.0, -30.0, dtype=np.complex64)
+    return V, probe, ps, dz, E
+
+
+def test_empty_inputs_raise(wap):
+    V, probe, ps, dz, E = _setup(64, 2)
+    H = wap.fresnel_propagation_kernel(64, 64, (ps, ps), dz, E)
+    with pytest.raises(ValueError):
+        wap.simulate_fresnel_as(V[:0], probe, H, dz, E)                      # no slices
+    with pytest.raises(ValueError):
+        wap.simulate_fresnel_as(V, probe, H, dz, E, positions=np.zeros((0, 2), np.int32))   # no probes
+    with pytest.raises(ValueError):
+        wap.simulate_fresnel_as(V, probe[:, :32], H, dz, E)                  # probe / potential grids differ
+    with pytest.raises(ValueError):
+        wap.simulate_fresnel_as(V, probe, H[:32], dz, E)                     # transfer function grid differs
+
+
+def test_largest_grid_single_probe(wap):
+    """2048^2, the largest grid of the transform kernels, against the FP64 oracle."""
+    from oracle import propagation_oracle as O
+    n, N = 2048, 2
+    V, probe, ps, dz, E = _setup(n, N, seed=3)
+    H = wap.angular_spectrum_propagation_kernel(n, n, (ps, ps), dz, E)
+    ex, dp, _ = wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)
+    rex, rdp, _ = O.simulate_fresnel_as(V.astype(np.float64), probe, H.cpu().numpy(), dz, E, return_wavefronts=False)
+    assert O.rel_l2(ex.cpu().numpy(), rex) < 1e-5
+    assert O.rel_l2(dp.cpu().numpy(), rdp) < 1e-5
+
+
+@pytest.mark.parametrize("B", [7, 8, 9])   # around the scheduler's threshold (8 probes)
+def test_wrapping_positions_both_paths(wap, B):
+    """Positions at and beyond the grid edges wrap like the reference's
+    jnp.roll (move_probe); 7 probes run the per-pass kernels, 8 and 9 the
+    persistent scheduler; every probe must equal its own single-probe run."""
+    from oracle import propagation_oracle as O
+    n = 128
+    V, probe, ps, dz, E = _setup(n, 3, seed=1)
+    H = wap.fresnel_propagation_kernel(n, n, (ps, ps), dz, E)
+    edge = np.array([[0, 0], [n - 1, n - 1], [0, n - 1], [n - 1, 0], [1, 64], [64, 127], [127, 1], [63, 0],
+                     [5, 5]], np.int32)[:B]
+    ex, dp, _ = wap.simulate_fresnel_as(V, probe, H, dz, E, positions=edge, return_wavefronts=False)
+    Ho = H.cpu().numpy()
+    for b in range(B):
+        p0 = O.move_probe(probe.astype(np.complex128), tuple(edge[b]))
+        rex, rdp, _ = O.simulate_fresnel_as(V.astype(np.float64), p0, Ho, dz, E, return_wavefronts=False)
+        assert O.rel_l2(ex[b].cpu().numpy(), rex) < 1e-5, b
+        assert O.rel_l2(dp[b].cpu().numpy(), rdp) < 1e-5, b
+
+
+def test_one_slice(wap):
+    from oracle import propagation_oracle as O
+    V, probe, ps, dz, E = _setup(256, 1, seed=2)
+    H = wap.fresnel_propagation_kernel(256, 256, (ps, ps), dz, E)
+    pos = np.array([[128, 128]] * 8 + [[3, 250]] * 8, np.int32)             # 16 probes: scheduler, one slice
+    ex, dp, _ = wap.simulate_fresnel_as(V, probe, H, dz, E, positions=pos, return_wavefronts=False)
+    for b in (0, 15):
+        p0 = O.move_probe(probe.astype(np.complex128), tuple(pos[b]))
+        rex, _, _ = O.simulate_fresnel_as(V.astype(np.float64), p0, H.cpu().numpy(), dz, E, return_wavefronts=False)
+        assert O.rel_l2(ex[b].cpu().numpy(), rex) < 1e-5
