@@ -98,6 +98,14 @@ int wap_multislice_fwd(wap_plan* plan, const float* V, int n_slices, int n_draws
                        const float* H_lo, double dz, double energy, float* exit, float* dp,
                        float* stack, void* stream);
 
+/* out[b] = ifft2(H X[b]) for n spectra X (complex64, (n, ny, nx)), H the plan
+ * grid's complex64 hi part and H_lo its remainder (or NULL): the inverse
+ * transform of wpm_propagation_kernel (propagation.py:159-167), whose H is
+ * exp(i dz sqrt(n^2 k0^2 - k_perp^2)) (build it with wap_line_transfer over the
+ * flattened k_perp^2).  out may equal X. */
+int wap_spectrum_propagate(wap_plan* plan, const float* X, int n, const float* H, const float* H_lo, float* out,
+                           void* stream);
+
 /* 1D helpers (propagation.py:609-652) and the naive per-pixel WPM step.
  *
  * wap_line_transfer: out (n) complex128 =

@@ -99,3 +99,24 @@ def test_binned_wpm_converges_to_naive(wap):
         assert abs(e - e_ref) < 0.1 * e_ref + 2e-6, (K, e, e_ref)
         errs.append(e)
     assert errs[0] > errs[1] > errs[2]
+
+
+def test_wpm_propagation_kernel_2d(wap):
+    """wpm_propagation_kernel(_vmap) (propagation.py:159-171) against the oracle,
+    with evanescent components (k_perp beyond n k0 at the grid corners)."""
+    from oracle import propagation_oracle as O
+    rng = np.random.default_rng(11)
+    ny, nx = 64, 128
+    Ek = np.fft.fft2(rng.normal(size=(ny, nx)) + 1j * rng.normal(size=(ny, nx)))
+    k0, dz = 30.0, 0.8
+    ky = 2 * np.pi * np.fft.fftfreq(ny, 0.1)
+    kx = 2 * np.pi * np.fft.fftfreq(nx, 0.1)
+    kp2 = ky[:, None] ** 2 + kx[None, :] ** 2
+    assert (kp2 > (1.3 * k0) ** 2).any()
+    ns = [1.0, 1.1, 1.3]
+    out = wap.wpm_propagation_kernel_vmap(Ek, ns, k0, kp2, dz)
+    for i, n in enumerate(ns):
+        assert rel(out[i], O.wpm_propagation_kernel(Ek, n, k0, kp2, dz)) < 1e-5
+    assert rel(wap.wpm_propagation_kernel(Ek, 1.1, k0, kp2, dz), O.wpm_propagation_kernel(Ek, 1.1, k0, kp2, dz)) < 1e-5
+    with pytest.raises(NotImplementedError):
+        wap.get_abtem_transmit(None, 300e3)

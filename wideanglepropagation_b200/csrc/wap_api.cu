@@ -595,6 +595,36 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
 
 extern "C" {
 
+int wap_spectrum_propagate(wap_plan* p, const float* X, int n, const float* H, const float* H_lo, float* out,
+                           void* stream) {
+  clear_error();
+  if (!p || !X || !H || !out) return fail(WAP_ERR_ARG, "NULL argument");
+  if (n < 1 || n > p->max_batch) return fail(WAP_ERR_ARG, "n=%d outside 1..%d (plan batch)", n, p->max_batch);
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long plane = (long long)p->ny * p->nx;
+  cudaError_t e;
+  if (out != X && (e = cudaMemcpyAsync(out, X, (size_t)n * plane * sizeof(float2), cudaMemcpyDeviceToDevice, st)) !=
+                      cudaSuccess)
+    return cuda_fail(e, "spectrum copy");
+  // columns: * H (hi + lo), inverse column FFT (no forward one)
+  ColArgs c = base_col_args(p, H, H_lo);
+  c.psi = reinterpret_cast<float2*>(out);
+  c.psi_bstride = plane;
+  c.flags = COL_NO_FFT;
+  if ((e = col_chunks(p, c, n, st)) != cudaSuccess) return cuda_fail(e, "spectrum column pass");
+  // rows: inverse row FFT and the 1/(ny nx) of ifft2
+  RowArgs r{};
+  r.psi = reinterpret_cast<float2*>(out);
+  r.psi_bstride = plane;
+  r.tw = p->tw_row;
+  r.ny = p->ny;
+  r.nx = p->nx;
+  r.flags = ROW_IFFT;
+  r.scale = (float)(1.0 / (double)plane);
+  if ((e = row_chunks(p, r, n, st)) != cudaSuccess) return cuda_fail(e, "spectrum row pass");
+  return WAP_OK;
+}
+
 int wap_multislice_fwd(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw, const float* psi0,
                        int n_probes, int psi0_per_probe, const int32_t* positions, const float* H, const float* H_lo,
                        double dz, double energy, float* exit, float* dp, float* stack, void* stream) {

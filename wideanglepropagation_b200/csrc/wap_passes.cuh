@@ -49,6 +49,7 @@ enum ColFlags : int {
   COL_DP = 2,         // write |H X|^2 (fftshifted) into dp
   COL_SEED = 4,       // adjoint seed: X <- n_px g X (+ fft of second buffer)
   COL_NO_H = 8,       // skip the propagator (pure 2D FFT epilogue)
+  COL_NO_FFT = 16,    // the tile is already a spectrum along y: no forward column FFT
 };
 
 struct RowArgs {
@@ -327,7 +328,7 @@ col_pass_kernel(const ColArgs a) {
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
 
-  fft<NY, E, false>(v, t, xs, tw);
+  if (!(f & COL_NO_FFT)) fft<NY, E, false>(v, t, xs, tw);
 
   // fftshift of (ky, kx) for dp / g
   const int sx = (col + (nx >> 1)) & (nx - 1);

@@ -46,6 +46,7 @@ __all__ = [
     "move_probe", "transmission_function", "simulate_fresnel_as",
     "simulate_fresnel_as_jit", "simulate_fresnel", "simulate_wpm",
     "simulate_wpm_jit", "max_angle_gpts", "downsample_to_max_angle", "detector_window",
+    "wpm_propagation_kernel", "wpm_propagation_kernel_vmap", "get_abtem_transmit",
 ]
 
 
@@ -491,6 +492,46 @@ def Propagator(u, H):
     V = torch.zeros((1, ny, nx), dtype=torch.float32, device=dev)
     out, _, _ = simulate_fresnel_as(V, u, H, 1.0, 100e3, return_wavefronts=False)
     return out
+
+
+def wpm_propagation_kernel_vmap(Ek, n_vals, k0, k_perp2, dz) -> torch.Tensor:
+    """ifft2(exp(i dz sqrt((n k0)^2 - k_perp^2)) Ek) for every n in ``n_vals``
+    (propagation.py:159-171): (len(n_vals), ny, nx) complex64.  The propagator
+    is evaluated in float64 and applied as complex64 hi + lo parts; the inverse
+    transform runs in the pass kernels."""
+    dev = _device()
+    X = _to(Ek, torch.complex64, dev)
+    if X.ndim != 2:
+        raise ValueError("Ek must be one (ny, nx) spectrum")
+    ny, nx = X.shape
+    kp2 = _to(k_perp2, torch.float64, dev).reshape(-1)
+    if kp2.numel() != ny * nx:
+        raise ValueError("k_perp2 must have the shape of Ek")
+    nv = np.atleast_1d(np.asarray(n_vals.cpu() if isinstance(n_vals, torch.Tensor) else n_vals, dtype=np.float64))
+    plan = get_plan(ny, nx, 1, _lib.WAP_OP_FRESNEL_AS)
+    out = torch.empty((nv.size, ny, nx), dtype=torch.complex64, device=dev)
+    H = torch.empty(ny * nx, dtype=torch.complex128, device=dev)
+    L = _lib.lib()
+    for i, n in enumerate(nv):
+        _lib.check(L.wap_line_transfer(_lib.WAP_TF_ANGULAR, ny * nx, _ptr(kp2), float(n) * float(k0), float(dz),
+                                       _ptr(H), _stream()))
+        Hh, Hl = split_transfer(H.view(ny, nx), dev)
+        _lib.check(L.wap_spectrum_propagate(plan.handle, _ptr(X), 1, _ptr(Hh), _ptr(Hl), _ptr(out[i]), _stream()))
+    return out
+
+
+def wpm_propagation_kernel(Ek, n_val, k0, k_perp2, dz) -> torch.Tensor:
+    """One homogeneous-index WPM propagate of a spectrum (propagation.py:159-167)."""
+    return wpm_propagation_kernel_vmap(Ek, [float(n_val)], k0, k_perp2, dz)[0]
+
+
+def get_abtem_transmit(potential, energy):
+    """propagation.py:286-299 builds transmission functions from abTEM
+    potential objects; abTEM is not part of this package.  Build the potential
+    with ``gaussian_potential`` (or pass a potential array to the simulators,
+    which form the transmission on the device)."""
+    raise NotImplementedError("get_abtem_transmit needs abTEM potentials; use gaussian_potential or pass a "
+                              "potential array to simulate_fresnel_as / simulate_wpm")
 
 
 def _potential_from_index(n_map: torch.Tensor, energy: float) -> torch.Tensor:
