@@ -241,12 +241,15 @@ int wap_scan_run(wap_scan* scan, void* stream);
  * sweeps the adjoint in reverse slice order, all in the persistent
  * scheduler.  dp must be non-NULL.  wap_scan_grad_backward accumulates
  * dL/dV (+=, laid out like V) for a loss whose gradient w.r.t. the
- * diffraction pattern is grad_dp (n_probes, n, n).  No counterpart function in
+ * diffraction pattern is grad_dp (n_probes, n, n), or (n_probes, det_ny,
+ * det_nx) with a detector window.  No counterpart function in
  * the reference (its paper claims autodiff through JAX, Paper/main.tex:271-274). */
 int wap_scan_grad_create(wap_scan** scan, const wap_scan_class* cls, int ckpt_every);
 int wap_scan_grad_backward(wap_scan* scan, const float* grad_dp, float* grad_V, void* stream);
-/* Re-point a scan at other buffers of the same shapes (no device allocation;
- * the column-tile tensor maps are re-encoded on the host). */
+/* Re-point a scan at other buffers of the same shapes (the column-tile tensor
+ * maps are re-encoded on the host; a class's detector window may change - the
+ * first window set on a class allocates its full-grid pattern scratch, nothing
+ * else is allocated). */
 int wap_scan_bind(wap_scan* scan, int n_classes, const wap_scan_class* classes);
 int wap_scan_status(wap_scan* scan, int* status);
 int wap_scan_info(const wap_scan* scan, long long* tickets, int* grid, int* group0);
