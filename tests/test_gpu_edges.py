@@ -80,3 +80,25 @@ def test_one_slice(wap):
         p0 = O.move_probe(probe.astype(np.complex128), tuple(pos[b]))
         rex, _, _ = O.simulate_fresnel_as(V.astype(np.float64), p0, H.cpu().numpy(), dz, E, return_wavefronts=False)
         assert O.rel_l2(ex[b].cpu().numpy(), rex) < 1e-5
+
+
+def test_release_caches_frees_and_recovers(wap):
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    V, probe, ps, dz, E = _setup(128, 3, seed=4)
+    H = wap.fresnel_propagation_kernel(128, 128, (ps, ps), dz, E)
+    pos = np.array([[i * 8, 100 - i * 5] for i in range(12)], np.int32)
+    ex0, _, _ = wap.simulate_fresnel_as(V, probe, H, dz, E, positions=pos, return_wavefronts=False)
+    Vt = torch.tensor(V, device="cuda", requires_grad=True)
+    _, dp = simulate_fresnel_as_differentiable(Vt, probe, H, dz, E, positions=pos)
+    dp.sum().backward()
+    g0 = Vt.grad.clone()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    wap.release_caches()
+    assert torch.cuda.mem_get_info()[0] >= free0      # plans, scans and pooled gradient scans gone
+    ex1, _, _ = wap.simulate_fresnel_as(V, probe, H, dz, E, positions=pos, return_wavefronts=False)
+    assert torch.equal(ex0, ex1)                      # rebuilt on demand, same numbers
+    Vt.grad = None
+    _, dp = simulate_fresnel_as_differentiable(Vt, probe, H, dz, E, positions=pos)
+    dp.sum().backward()
+    assert float((Vt.grad - g0).norm() / g0.norm()) < 1e-6

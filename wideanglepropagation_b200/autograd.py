@@ -48,9 +48,27 @@ def _acquire(key, cls, k):
     return h
 
 
+_POOL_IDLE_MAX = 2   # idle gradient scans kept per shape (each holds its checkpoints and segment waves)
+
+
 def _release(key, h):
     with _pool_lock:
-        _pool.setdefault(key, []).append(h)
+        free = _pool.setdefault(key, [])
+        if len(free) < _POOL_IDLE_MAX:
+            free.append(h)
+            return
+    _lib.lib().wap_scan_destroy(h)
+
+
+def release_pool() -> None:
+    """Destroy every idle pooled gradient scan (scans held by pending graphs stay)."""
+    with _pool_lock:
+        handles = [h for free in _pool.values() for h in free]
+        _pool.clear()
+    if handles:
+        torch.cuda.synchronize()
+        for h in handles:
+            _lib.lib().wap_scan_destroy(h)
 
 
 class _Lease:

@@ -46,7 +46,7 @@ __all__ = [
     "move_probe", "transmission_function", "simulate_fresnel_as",
     "simulate_fresnel_as_jit", "simulate_fresnel", "simulate_wpm",
     "simulate_wpm_jit", "max_angle_gpts", "downsample_to_max_angle", "detector_window",
-    "wpm_propagation_kernel", "wpm_propagation_kernel_vmap", "get_abtem_transmit",
+    "wpm_propagation_kernel", "wpm_propagation_kernel_vmap", "get_abtem_transmit", "release_caches",
 ]
 
 
@@ -397,6 +397,23 @@ def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None):
         else:
             _lib.check(L.wap_scan_bind(h, 1, arr))
         _lib.check(L.wap_scan_run(h, _stream()))
+
+
+def release_caches() -> None:
+    """Free the device memory the library keeps between calls: cached plans
+    (twiddles, WPM workspaces), cached forward scans (transmission tables,
+    interleaved propagators) and idle pooled gradient scans."""
+    torch.cuda.synchronize()
+    with _scans_lock:
+        for h in _scans.values():
+            _lib.lib().wap_scan_destroy(h)
+        _scans.clear()
+    with _plans_lock:
+        for p in _plans.values():
+            p.close()
+        _plans.clear()
+    from . import autograd
+    autograd.release_pool()
 
 
 def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, *,
