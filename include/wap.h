@@ -246,6 +246,12 @@ int wap_scan_run(wap_scan* scan, void* stream);
  * the reference (its paper claims autodiff through JAX, Paper/main.tex:271-274). */
 int wap_scan_grad_create(wap_scan** scan, const wap_scan_class* cls, int ckpt_every);
 int wap_scan_grad_backward(wap_scan* scan, const float* grad_dp, float* grad_V, void* stream);
+/* The same for a loss on the diffraction pattern and/or on the exit wave:
+ * grad_exit (n_probes, n, n) complex64 in the torch convention (dL/dRe +
+ * i dL/dIm), either pointer may be NULL (not both).  The exit-wave term enters
+ * the seed as fft2(grad_exit / 2), formed with the pass kernels first. */
+int wap_scan_grad_backward_ex(wap_scan* scan, const float* grad_dp, const float* grad_exit, float* grad_V,
+                              void* stream);
 /* Re-point a scan at other buffers of the same shapes (the column-tile tensor
  * maps are re-encoded on the host; a class's detector window may change - the
  * first window set on a class allocates its full-grid pattern scratch, nothing

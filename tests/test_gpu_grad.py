@@ -167,3 +167,31 @@ def test_persistent_gradient_two_pending_graphs(wap):
     (((d1 - tr) ** 2).sum() + ((d2 - tr) ** 2).sum()).backward()
     err = np.linalg.norm(V.grad.cpu().numpy() - Vr.grad.numpy()) / np.linalg.norm(Vr.grad.numpy())
     assert err < 1e-4, err
+
+
+@pytest.mark.parametrize("ckpt,dp_weight", [(3, 1e-3), (9, 1e-3), (2, 0.0)])
+def test_persistent_gradient_exit_wave_loss(wap, ckpt, dp_weight):
+    """A loss on the exit wave through the persistent scheduler: the seed adds
+    fft2(dL/d(exit) / 2) to the diffraction term (or stands alone when the
+    loss ignores the pattern).  Tolerance 5e-4 as for the per-pass case."""
+    from oracle import torch_oracle as T
+    from wideanglepropagation_b200.autograd import SCAN_MIN_PROBES, simulate_fresnel_as_differentiable
+    V0, probe, pos, H, dz, E, target = _scan_problem(N=7, seed=8)
+    assert len(pos) >= SCAN_MIN_PROBES
+    n = V0.shape[-1]
+    rng = np.random.default_rng(2)
+    c = rng.normal(size=(len(pos), n, n)) + 1j * rng.normal(size=(len(pos), n, n))
+    Vr = torch.tensor(V0, requires_grad=True)
+    ex_r, dp_r = T.simulate(Vr, probe, H, dz, E, pos)
+    Lr = (ex_r * torch.tensor(c)).real.sum()
+    if dp_weight:
+        Lr = Lr + dp_weight * (dp_r ** 2).sum()
+    Lr.backward()
+    V = torch.tensor(V0, dtype=torch.float32, device="cuda", requires_grad=True)
+    ex, dp = simulate_fresnel_as_differentiable(V, probe, H, dz, E, positions=pos, ckpt_every=ckpt)
+    L = (ex * torch.tensor(c, dtype=torch.complex64, device="cuda")).real.sum()
+    if dp_weight:
+        L = L + dp_weight * (dp.double() ** 2).sum()
+    L.backward()
+    err = np.linalg.norm(V.grad.cpu().numpy() - Vr.grad.numpy()) / np.linalg.norm(Vr.grad.numpy())
+    assert err < 5e-4, err

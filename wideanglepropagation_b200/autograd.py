@@ -137,21 +137,19 @@ class MultisliceFunction(torch.autograd.Function):
     def backward(ctx, g_exit, g_dp):
         if ctx.scan is not None:
             lease = ctx.scan
-            h = lease.h
             Vc, _ = ctx.saved_tensors
             B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta
             try:
-                if g_exit is None and g_dp is not None:
-                    grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=Vc.device)
-                    g = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
-                    _lib.check(_lib.lib().wap_scan_grad_backward(h, _ptr(g), _ptr(grad_V), _stream()))
+                grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=Vc.device)
+                if g_exit is None and g_dp is None:
                     return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
+                g = None if g_dp is None else g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
+                ge = None if g_exit is None else g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
+                _lib.check(_lib.lib().wap_scan_grad_backward_ex(lease.h, _ptr(g), _ptr(ge), _ptr(grad_V),
+                                                                _stream()))
+                return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
             finally:
                 lease.release()
-            # a loss on the exit wave: the per-pass adjoint below needs its own checkpoints
-            psi, pos, dr, Hc, Hl = ctx.keep
-            return _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp,
-                                      det)
         Vc, Hc, Hl, exit_wave, ckpt, dr = ctx.saved_tensors
         B, N, ny, nx, dz, energy, k, has_draw, vshape, batched, det = ctx.meta
         dev = Vc.device
@@ -168,30 +166,6 @@ class MultisliceFunction(torch.autograd.Function):
             _ptr(Hl) if Hl.numel() else None, dz, energy,
             _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
         return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
-
-
-def _per_pass_backward(Vc, psi, pos, dr, Hc, Hl, dz, energy, k, B, N, ny, nx, vshape, g_exit, g_dp, det):
-    """Checkpointed forward + hand-written adjoint with the per-pass kernels."""
-    dev = Vc.device
-    plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
-    plan.set_detector(det)
-    nck = (N + k - 1) // k
-    exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
-    dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
-    ckpt = torch.empty((B, nck, ny, nx), dtype=torch.complex64, device=dev)
-    _lib.check(_lib.lib().wap_multislice_fwd_ckpt(
-        plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), _ptr(psi), B, 0, _ptr(pos), _ptr(Hc), _ptr(Hl),
-        dz, energy, _ptr(exit_wave), _ptr(dp), _ptr(ckpt), k, _stream()))
-    if g_exit is not None:
-        g_exit = g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
-    if g_dp is not None:
-        g_dp = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
-    grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=dev)
-    work = torch.empty((B, k + 2, ny, nx), dtype=torch.complex64, device=dev)
-    _lib.check(_lib.lib().wap_multislice_bwd(
-        plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), B, _ptr(Hc), _ptr(Hl), dz, energy,
-        _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
-    return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
 
 
 def simulate_fresnel_as_differentiable(potential: torch.Tensor, probe, prop_kernel, slice_thickness, energy, *,

@@ -50,6 +50,7 @@ enum ColFlags : int {
   COL_SEED = 4,       // adjoint seed: X <- n_px g X (+ fft of second buffer)
   COL_NO_H = 8,       // skip the propagator (pure 2D FFT epilogue)
   COL_NO_FFT = 16,    // the tile is already a spectrum along y: no forward column FFT
+  COL_FWD_ONLY = 32,  // store the spectrum after the forward FFT (and H): no inverse FFT
 };
 
 struct RowArgs {
@@ -394,7 +395,7 @@ col_pass_kernel(const ColArgs a) {
     if (f & COL_NO_H) return;  // pure diffraction epilogue: no inverse transform
   }
 
-  fft<NY, E, true>(v, t, xs, tw);
+  if (!(f & COL_FWD_ONLY)) fft<NY, E, true>(v, t, xs, tw);
 
   __syncthreads();
 #pragma unroll

@@ -125,7 +125,8 @@ struct SchedClass {
   int ckpt_n, seg_n;            // slots per probe
   int ckpt_k;                   // gradient scans: checkpoint every ckpt_k slices (0: none)
   int seg_first;                // first slice of the trailing segments the forward keeps
-  const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp (full grid)
+  const float* g;               // (B, n, n) dL/d(dp), fftshifted like dp (full grid; zeros for an exit-only loss)
+  const float2* seed_add;       // (B, n, n) spectrum added to the seed (exit-wave loss), or null
   float* grad;                  // (draws, N, n, n) probe sums of Re(conj(lambda_a) i a_s)
   float ri_a, ri_inv_den, kphase, e_plus_e0;
   const float4* tw;             // twiddles for (n, E) in global memory
@@ -482,11 +483,17 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     if (type == ST_SEED_COL) {
       // lambda seed: n^2 g Z with g = dL/d(dp) at the fftshifted position
       // (zero outside the detector window)
+      // (+ the exit-wave loss's seed: fft2(dL/d(exit) / 2) at (ky, kx))
       const float* gp = c.g + (long long)k.b * plane;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int sy = (t + T * e + (N >> 1)) & (N - 1);
         v[e] = cscale(v[e], c.inv_scale * __ldg(gp + (long long)sy * N + sx));
+      }
+      if (c.seed_add) {
+        const float2* sp = c.seed_add + (long long)k.b * plane + col;
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = cadd(v[e], __ldcg(sp + (long long)(t + T * e) * N));
       }
     }
   }
@@ -1313,14 +1320,23 @@ static int scan_launch(wap_scan* s, bool backward, cudaStream_t st) {
   if (backward) {
     params.stage2 = s->psi_mode;
     params.cls[0].grad = s->d_gsum;
-    if (windowed(s->det[0], s->cls[0].n)) {
-      // the seed reads a full-grid dL/d(dp): zero outside the window
-      const wap_scan_class& c = s->cls[0];
-      const long long total = (long long)c.n_probes * c.n * c.n;
-      count_launch();
-      scatter_window_kernel<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, st>>>(
-          s->params.cls[0].g, s->d_dpfull[0], total, c.n, s->det[0]);
-      if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scatter_window_kernel");
+    const wap_scan_class& c = s->cls[0];
+    const long long total = (long long)c.n_probes * c.n * c.n;
+    const bool no_dp = !s->params.cls[0].g;   // a loss on the exit wave alone: the seed reads g = 0
+    if (no_dp || windowed(s->det[0], c.n)) {
+      if (s->d_dpfull.empty()) s->d_dpfull.resize(1, nullptr);
+      if (!s->d_dpfull[0] && (e = cudaMalloc(&s->d_dpfull[0], total * sizeof(float))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(full-grid seed scratch)");
+      if (no_dp) {
+        if ((e = cudaMemsetAsync(s->d_dpfull[0], 0, total * sizeof(float), st)) != cudaSuccess)
+          return cuda_fail(e, "seed scratch reset");
+      } else {
+        // the seed reads a full-grid dL/d(dp): zero outside the window
+        count_launch();
+        scatter_window_kernel<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, st>>>(
+            s->params.cls[0].g, s->d_dpfull[0], total, c.n, s->det[0]);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "scatter_window_kernel");
+      }
       params.cls[0].g = s->d_dpfull[0];
     }
     if ((e = cudaMemsetAsync(s->d_gsum, 0, s->ttab_elems[0] * sizeof(float), st)) != cudaSuccess)
@@ -1466,10 +1482,57 @@ int wap_scan_run(wap_scan* s, void* stream) {
 int wap_scan_grad_backward(wap_scan* s, const float* grad_dp, float* grad_V, void* stream) {
   clear_error();
   if (!s || !grad_dp || !grad_V) return fail(WAP_ERR_ARG, "NULL argument");
+  return wap_scan_grad_backward_ex(s, grad_dp, nullptr, grad_V, stream);
+}
+
+int wap_scan_grad_backward_ex(wap_scan* s, const float* grad_dp, const float* grad_exit, float* grad_V,
+                              void* stream) {
+  clear_error();
+  if (!s || !grad_V || (!grad_dp && !grad_exit)) return fail(WAP_ERR_ARG, "need grad_V and grad_dp or grad_exit");
   if (!s->grad) return fail(WAP_ERR_ARG, "scan was not created for gradients");
-  s->params.cls[0].g = grad_dp;
-  s->params.cls[0].grad = grad_V;
-  return scan_launch(s, true, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  SchedClass& sc = s->params.cls[0];
+  const wap_scan_class& c = s->cls[0];
+  sc.g = grad_dp;
+  sc.grad = grad_V;
+  sc.seed_add = nullptr;
+  if (grad_exit) {
+    // fft2(grad_exit / 2) into the recompute buffer (free until the first
+    // recompute, which the seed precedes in every probe's chain), with the
+    // pass kernels and the scan's twiddles; the seed column step adds it
+    const int n = c.n, E = 16, T = n / E;
+    const long long plane = (long long)n * n;
+    RowArgs r{};
+    r.psi = sc.work;
+    r.psi_bstride = plane;
+    r.src = reinterpret_cast<const float2*>(grad_exit);
+    r.src_bstride = plane;
+    r.tw = sc.tw;
+    r.ny = n;
+    r.nx = n;
+    r.flags = ROW_LOAD_SRC | ROW_FFT | ROW_SCALE_SRC;
+    r.scale = 1.0f;
+    r.src_scale = 0.5f;
+    ColArgs cc{};
+    cc.psi = sc.work;
+    cc.psi_bstride = plane;
+    cc.tw = sc.tw;
+    cc.ny = n;
+    cc.nx = n;
+    cc.flags = COL_NO_H | COL_FWD_ONLY;
+    cc.det = Detector{0, 0, n, n};
+    const int col_w = std::max(2, std::min(16, kColThreads / T));
+    cudaError_t e;
+    for (int b0 = 0; b0 < c.n_probes; b0 += 65535) {
+      const int nb = std::min(65535, c.n_probes - b0);
+      r.probe0 = b0;
+      cc.probe0 = b0;
+      if ((e = launch_row(n, E, r, nb, rows_per_cta(n, E, n), st)) != cudaSuccess) return cuda_fail(e, "exit seed rows");
+      if ((e = launch_col(n, E, cc, nb, col_w, st)) != cudaSuccess) return cuda_fail(e, "exit seed columns");
+    }
+    sc.seed_add = sc.work;
+  }
+  return scan_launch(s, true, st);
 }
 
 int wap_scan_status(wap_scan* s, int* status) {
