@@ -16,6 +16,7 @@ Printed JSON line (rank 0):
   grad_over_fwd  t(forward + adjoint gradient) / t(forward) on the
               512^2, 64-slice, 64-probe inverse problem (checkpoint every 8)
   err_vs_fp64 rel-L2 of exit wave and diffraction pattern vs the FP64 oracle
+              (probe 0 of each grid class, as the headline scan left them)
   roofline    dominant pass kernel: algorithmic bytes / device time vs the
               measured HBM copy bandwidth
   cpu_baseline  the NumPy/SciPy FP64 restatement on the host cores
@@ -295,11 +296,12 @@ def main():
     # the others would idle at the next collective while rank 0 runs them
     extras_on = not args.no_extras and world == 1
     if extras_on:
+        # first: the exit waves are still the headline scan's (the per-pass leg rewrites them)
+        extras.update(_err_vs_fp64(classes, classes_host))
         extras.update(_plain(classes, args))
         extras.update(_per_pass(classes, args))
         extras.update(_configs())
         extras.update(_grad_ratio(args))
-        extras.update(_err_vs_fp64(classes, classes_host))
         extras.update(_lines())
         extras.update(_potential_builder())
         extras.update(_lippmann_schwinger())

@@ -12,7 +12,9 @@
 //   twiddle W_{LR}^{jk}, from a per-stage table laid out [j][k] so that
 //           consecutive threads read consecutive words; each entry holds
 //           the float64 value as float hi + lo parts (systematic rounding
-//           of a float-only table would repeat identically every slice)
+//           of a float-only table would repeat identically every slice);
+//           the hi parts alone (float2) are the cheaper format for waves
+//           that pass through few enough transforms
 //   outputs y_m -> position (b - k) R + k + m L, exchanged through shared
 //           memory for every stage but the last.
 // After the last stage thread t again holds X[t + T*e] in slot e, so a forward
@@ -169,6 +171,15 @@ __device__ __forceinline__ float2 cmulc_tw(float2 a, float4 w) {
   return make_float2(fmaf(a.x, w.x, fmaf(a.y, w.y, fmaf(a.x, w.z, a.y * w.w))),
                      fmaf(a.y, w.x, fmaf(-a.x, w.y, fmaf(a.y, w.z, -a.x * w.w))));
 }
+// stage-twiddle multiply for the two table formats: float4 (hi + lo, exact to
+// float64 rounding) or float2 (hi only: one rounding per entry, which repeats
+// identically in every transform - cheaper, with a systematic error that grows
+// with the number of transforms a wave goes through)
+template <bool INV>
+__device__ __forceinline__ float2 tw_mul(float2 a, float4 w) { return INV ? cmulc_tw(a, w) : cmul_tw(a, w); }
+template <bool INV>
+__device__ __forceinline__ float2 tw_mul(float2 a, float2 w) { return INV ? cmulc(a, w) : cmul(a, w); }
+
 // a * (h + hl) for a propagator value split into complex64 hi and lo parts
 __device__ __forceinline__ float2 cmul_hl(float2 a, float2 h, float2 hl) {
   return make_float2(fmaf(a.x, h.x, fmaf(-a.y, h.y, fmaf(a.x, hl.x, -a.y * hl.y))),
@@ -291,8 +302,8 @@ struct ColExchange {
 // ----------------------------------------------------------------------------
 // Stockham stages
 // ----------------------------------------------------------------------------
-template <int N, int E, int SI, bool INV, class X>
-__device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, const float4* __restrict__ tw) {
+template <int N, int E, int SI, bool INV, class X, class TW>
+__device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, const TW* __restrict__ tw) {
   using P = FFTPlan<N, E>;
   constexpr int R = P::radix(SI);
   constexpr int L = P::span(SI);
@@ -310,8 +321,7 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
     if constexpr (L > 1) {
 #pragma unroll
       for (int j = 1; j < R; ++j) {
-        const float4 w = tw[OFF + (j - 1) * L + k];
-        a[j] = INV ? cmulc_tw(a[j], w) : cmul_tw(a[j], w);
+        a[j] = tw_mul<INV>(a[j], tw[OFF + (j - 1) * L + k]);
       }
     }
     dft<R, INV>(a);
@@ -334,8 +344,9 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
   }
 }
 
-template <int N, int E, bool INV, class X, int SI = 0>
-__device__ __forceinline__ void fft(float2 (&v)[E], int t, const X& xs, const float4* __restrict__ tw) {
+// TW: float4 (hi + lo) or float2 (hi only) stage-twiddle table
+template <int N, int E, bool INV, class X, int SI = 0, class TW>
+__device__ __forceinline__ void fft(float2 (&v)[E], int t, const X& xs, const TW* __restrict__ tw) {
   if constexpr (SI < FFTPlan<N, E>::S) {
     fft_stage<N, E, SI, INV>(v, t, xs, tw);
     fft<N, E, INV, X, SI + 1>(v, t, xs, tw);

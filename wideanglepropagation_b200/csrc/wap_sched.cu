@@ -53,6 +53,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "wap_internal.h"
@@ -322,6 +323,8 @@ __device__ __forceinline__ void issue_load(const SchedParams& P, const Task& k, 
 
 constexpr int kComputeWarps = kSchedThreads / 32;      // 8 compute warps
 constexpr int kBlockThreads = kSchedThreads + 32;       // + 1 producer warp
+// forward scans of at most this many slices use hi-only stage twiddles
+constexpr int kHiTwiddleMaxSlices = 160;
 constexpr int kFftBar = 2;                              // named barrier of the compute warps
 
 // ---------------------------------------------------------------------------
@@ -357,9 +360,9 @@ __device__ __forceinline__ void row_load(const SchedClass& c, const Task& k, int
 // are powers of two, so no rounding changes.  The forward instance (!GRAD)
 // runs the forward chain - with checkpoint / segment snapshots in gradient
 // scans - and the gradient instance runs the backward chain.
-template <int N, int E, bool GRAD, class Acquire, class Release>
+template <int N, int E, bool GRAD, class TW, class Acquire, class Release>
 __device__ __forceinline__ void row_compute(const SchedClass& c, const Task& k, const Step& st, float2 (&v)[E],
-                                            float2* exch, const float4* tw, const float2* stage2,
+                                            float2* exch, const TW* tw, const float2* stage2,
                                             const Acquire& acquire, const Release& release) {
   constexpr int T = N / E;
   constexpr int PADN = RowExchange<true>::padded(N);
@@ -467,9 +470,9 @@ __device__ __forceinline__ void col_load(const float2* stage, float2 (&v)[E]) {
 }
 
 // Column tile: FFT, * H or conj(H) (hi + lo), [dp / adjoint seed], inverse FFT.
-template <int N, int E, bool GRAD>
+template <int N, int E, bool GRAD, class TW>
 __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, const Step& st, float2 (&v)[E],
-                                            float2* exch, const float4* tw) {
+                                            float2* exch, const TW* tw) {
   constexpr int T = N / E;
   constexpr int W = kSchedThreads / T;
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
@@ -529,7 +532,8 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
 
 // Compute warps: take the published tile, pull it into registers, release the
 // stage, run the transforms, store, report completion.
-template <unsigned MASK, int E, bool GRAD>
+// HI_TW: the stage twiddles are hi parts only (float2 entries; tw_off counts them)
+template <unsigned MASK, int E, bool GRAD, bool HI_TW>
 __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage, float2* exch, const float4* tw_smem,
                                              uint64_t* full, uint64_t* empty, uint64_t* done_bar, const Task* s_task) {
   uint32_t fph = 0;
@@ -556,7 +560,8 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
     }
     const SchedClass& c = P.cls[k.cls];
     const Step st = step_of<GRAD>(c, k.pass);
-    const float4* tw = P.tw_in_smem ? tw_smem + c.tw_off : c.tw;
+    using TW = typename std::conditional<HI_TW, float2, float4>::type;
+    const TW* tw = P.tw_in_smem ? reinterpret_cast<const TW*>(tw_smem) + c.tw_off : reinterpret_cast<const TW*>(c.tw);
     const bool col = step_is_col(st.type);
     // Adjoint rows read psi_s next to lambda.  kPsiStage2: both arrive
     // together (second stage), released after psi_s is read.  kPsiSplit:
@@ -608,7 +613,7 @@ __device__ __forceinline__ void compute_loop(const SchedParams& P, float2* stage
 // ---------------------------------------------------------------------------
 // the persistent kernel: 8 compute warps + 1 producer warp
 // ---------------------------------------------------------------------------
-template <unsigned MASK, int E, bool GRAD>
+template <unsigned MASK, int E, bool GRAD, bool HI_TW = false>
 __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(const __grid_constant__ SchedParams P) {
   extern __shared__ __align__(1024) unsigned char sched_smem[];
   float2* stage = reinterpret_cast<float2*>(sched_smem);
@@ -632,7 +637,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   __syncthreads();
 
   if (threadIdx.x < kSchedThreads) {
-    compute_loop<MASK, E, GRAD>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
+    compute_loop<MASK, E, GRAD, HI_TW>(P, stage, exch, tw_smem, &full, &empty, done_bar, &s_task);
     return;
   }
 
@@ -824,12 +829,23 @@ static ScanKernel pick_fwd_e(unsigned mask) {
     default: return scan_kernel<15u, E, false>;
   }
 }
+static ScanKernel pick_fwd_hi(unsigned mask) {
+  switch (mask) {
+    case 1u: return scan_kernel<1u, 16, false, true>;
+    case 2u: return scan_kernel<2u, 16, false, true>;
+    case 4u: return scan_kernel<4u, 16, false, true>;
+    case 8u: return scan_kernel<8u, 16, false, true>;
+    case 6u: return scan_kernel<6u, 16, false, true>;
+    default: return scan_kernel<15u, 16, false, true>;
+  }
+}
+template <bool HI_TW>
 static ScanKernel pick_grad(unsigned mask) {
   switch (mask) {
-    case 1u: return scan_kernel<1u, 16, true>;
-    case 2u: return scan_kernel<2u, 16, true>;
-    case 4u: return scan_kernel<4u, 16, true>;
-    default: return scan_kernel<8u, 16, true>;
+    case 1u: return scan_kernel<1u, 16, true, HI_TW>;
+    case 2u: return scan_kernel<2u, 16, true, HI_TW>;
+    case 4u: return scan_kernel<4u, 16, true, HI_TW>;
+    default: return scan_kernel<8u, 16, true, HI_TW>;
   }
 }
 
@@ -838,6 +854,7 @@ struct wap_scan {
   ScanKernel kernel_bwd = nullptr;   // backward chain of gradient scans
   bool grad = false;
   int e = 16;
+  bool hi_tw = false;                // stage twiddles as hi parts only (forward scans of few slices)
   int device = 0;
   int n_classes = 0;
   SchedParams params{};
@@ -862,6 +879,7 @@ struct wap_scan {
   float* d_gsum = nullptr;          // (draws, N, n, n) probe sums of the adjoint sweep
   int ckpt_every = 0;
   std::vector<float4*> d_tw;
+  float4* d_tw_seed = nullptr;      // gradient scans: the hi + lo (n, 16) table of the exit-wave seed passes
   std::vector<float2*> d_ttab;
   std::vector<float4*> d_hq;
   std::vector<void*> d_extra;       // gradient buffers
@@ -893,6 +911,7 @@ static void scan_free(wap_scan* s) {
   cudaFree(s->d_status);
   cudaFree(s->d_debug);
   for (auto p : s->d_tw) cudaFree(p);
+  cudaFree(s->d_tw_seed);
   for (auto p : s->d_ttab) cudaFree(p);
   for (auto p : s->d_hq) cudaFree(p);
   for (auto p : s->d_extra) cudaFree(p);
@@ -1067,6 +1086,15 @@ static int upload(T** dst, const std::vector<T>& src, const char* what) {
   return e == cudaSuccess ? WAP_OK : cuda_fail(e, what);
 }
 
+// Stage-twiddle table of the hi-only instance: the float2 hi parts packed two
+// to a float4 entry (so the image and its prefix sharing work unchanged).
+static std::vector<float4> pack_hi(const std::vector<float4>& t) {
+  std::vector<float4> q((t.size() + 1) / 2, make_float4(0.f, 0.f, 0.f, 0.f));
+  float2* qp = reinterpret_cast<float2*>(q.data());
+  for (size_t i = 0; i < t.size(); ++i) qp[i] = make_float2(t[i].x, t[i].y);
+  return q;
+}
+
 // Shared set-up of forward scans (ckpt_every = 0) and gradient scans.
 static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes, int ckpt_every) {
   PFN_cuTensorMapEncodeTiled_v12000 encode = get_encode();
@@ -1086,6 +1114,20 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     if (!strcmp(ov, "8") && !s->grad) E = 8;
   }
   s->e = E;
+  // Hi-only stage twiddles: each entry's float rounding repeats in every
+  // transform, so its error grows linearly with the slices a wave crosses
+  // (measured on one B200: 4.5e-6 exit-wave error against the float64 oracle
+  // at 512^2 x 150 slices, 2.4e-6 with hi + lo; at most 4.9e-6 on 128^2 to
+  // 1024^2 grids up to 160 slices); about 10 % faster.  Scans of at most
+  // kHiTwiddleMaxSlices slices take them, in the forward and the backward
+  // chain alike, so a gradient scan's recompute reproduces its forward waves.
+  int max_slices = 0;
+  for (int ci = 0; ci < n_classes; ++ci) max_slices = std::max(max_slices, classes[ci].n_slices);
+  s->hi_tw = E == 16 && max_slices <= kHiTwiddleMaxSlices;
+  if (const char* ov = getenv("WAP_SCHED_TW")) {   // A/B timing and error checks only
+    if (!strcmp(ov, "full")) s->hi_tw = false;
+    if (!strcmp(ov, "hi")) s->hi_tw = E == 16;
+  }
   unsigned mask = 0;
   for (int ci = 0; ci < n_classes; ++ci) {
     const int n = classes[ci].n;
@@ -1102,6 +1144,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     std::vector<int> order(n_classes);
     for (int ci = 0; ci < n_classes; ++ci) {
       tables[ci] = twiddle_table(classes[ci].n, E);
+      if (s->hi_tw) tables[ci] = pack_hi(tables[ci]);
       order[ci] = ci;
     }
     std::stable_sort(order.begin(), order.end(),
@@ -1122,8 +1165,8 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     }
   }
   const int tw_total = (int)image.size();
-  s->kernel = E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask);
-  if (s->grad) s->kernel_bwd = pick_grad(mask);
+  s->kernel = s->hi_tw ? pick_fwd_hi(mask) : E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask);
+  if (s->grad) s->kernel_bwd = s->hi_tw ? pick_grad<true>(mask) : pick_grad<false>(mask);
   // Keep the twiddles in shared memory only when they fit next to the stage
   // and exchange buffers without lowering the CTAs per SM.
   const size_t base_smem = kTileBytesFor(E) + kExchBytesFor(E);
@@ -1216,7 +1259,11 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     if ((rc = upload(&dtw, h, "twiddle upload")) != WAP_OK) return rc;
     s->d_tw.push_back(dtw);
     sc.tw = dtw;
-    sc.tw_off = image_off[ci];
+    // the pass kernels that form an exit-wave seed read float4 hi + lo entries,
+    // whichever table format the scan itself uses
+    if (s->grad && ci == 0 && (rc = upload(&s->d_tw_seed, twiddle_table(n, E), "twiddle upload")) != WAP_OK)
+      return rc;
+    sc.tw_off = image_off[ci] * (s->hi_tw ? 2 : 1);   // in table entries (float2 for hi-only)
     sc.tw_len = (int)h.size();
     const size_t tt = (size_t)c.n_draws * c.n_slices * n * n;
     float2* dtt = nullptr;
@@ -1507,7 +1554,7 @@ int wap_scan_grad_backward_ex(wap_scan* s, const float* grad_dp, const float* gr
     r.psi_bstride = plane;
     r.src = reinterpret_cast<const float2*>(grad_exit);
     r.src_bstride = plane;
-    r.tw = sc.tw;
+    r.tw = s->d_tw_seed;
     r.ny = n;
     r.nx = n;
     r.flags = ROW_LOAD_SRC | ROW_FFT | ROW_SCALE_SRC;
@@ -1516,7 +1563,7 @@ int wap_scan_grad_backward_ex(wap_scan* s, const float* grad_dp, const float* gr
     ColArgs cc{};
     cc.psi = sc.work;
     cc.psi_bstride = plane;
-    cc.tw = sc.tw;
+    cc.tw = s->d_tw_seed;
     cc.ny = n;
     cc.nx = n;
     cc.flags = COL_NO_H | COL_FWD_ONLY;
