@@ -287,6 +287,17 @@ def main():
                 "traffic": _ncu_traffic(dom), "kernel": dom, "peak_source": peak_src,
                 "launches": n, "avg_launch_us": 1e3 * kms / n,
                 "share": {k: v[1] / sum(x[1] for x in kinds.values()) for k, v in kinds.items()}}
+    # FP32 side: algorithmic flops of one launch (10 N log2 N + 24 N per
+    # slice-step of an N-pixel Fresnel/AS grid) against the measured FMA peak;
+    # time_frac = max(bytes / HBM peak, flops / FP32 peak) / launch time
+    fp32_peak = _fp32_peak()
+    flops = sum(w.n_probes * w.n_slices * (10.0 * w.ny * w.nx * np.log2(w.ny * w.nx) + 24.0 * w.ny * w.nx)
+                for w in classes_host)
+    launch_s = kms / n / 1e3
+    roofline["fp32"] = {"achieved": flops / launch_s / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+                        "frac": flops / launch_s / 1e12 / fp32_peak, "flops_per_launch": flops,
+                        "peak_source": "FMA probe (wap_fp32_probe) in this run"}
+    roofline["time_frac"] = max(by / n / (peak * 1e9), flops / (fp32_peak * 1e12)) / launch_s
 
     if scan.sched is not None:
         st = scan.sched.status()
@@ -577,6 +588,34 @@ def _grad_ratio(args):
         out[k] = s.elapsed_time(e) / reps / t_f
     return {"grad_over_fwd": out[8], "grad_over_fwd_ckpt1": out[1], "grad_fwd_ms": t_f,
             "grad_workload": "512^2, 64 slices x 2 A, 300 keV, 64 probes (8x8), L = sum(|FFT psi|^2 - I)^2"}
+
+
+def _fp32_peak():
+    """FP32 FMA throughput (TFLOP/s) of this GPU: 8 CTAs of 256 threads per SM,
+    each thread 2^14 x 8 independent FMAs; best of five after three warm-ups."""
+    import ctypes
+    import torch
+    from wideanglepropagation_b200 import _lib
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    blocks, iters = sms * 8, 1 << 14
+    out = torch.empty(blocks * 256, dtype=torch.float32, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def launch():
+        _lib.check(_lib.lib().wap_fp32_probe(blocks, iters, ctypes.c_void_p(out.data_ptr()), stream))
+
+    for _ in range(3):
+        launch()
+    best = None
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        launch()
+        e.record()
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3
+        best = t if best is None else min(best, t)
+    return blocks * 256 * iters * 8 * 2 / best / 1e12
 
 
 def _peak_hbm():

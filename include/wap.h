@@ -289,6 +289,12 @@ int wap_profile_enable(int on);
 int wap_profile_reset(void);
 int wap_profile_read(int kind, long long* launches, double* total_ms, double* total_bytes);
 
+/* FP32 peak probe for the roofline (no counterpart in the reference):
+ * `blocks` CTAs of 256 threads, each thread `iters` x 8 independent FMAs
+ * (2 flops each), one float per thread written to `out` (blocks x 256).
+ * The caller times the launch on `stream`. */
+int wap_fp32_probe(int blocks, int iters, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,3 +102,23 @@ def test_release_caches_frees_and_recovers(wap):
     _, dp = simulate_fresnel_as_differentiable(Vt, probe, H, dz, E, positions=pos)
     dp.sum().backward()
     assert float((Vt.grad - g0).norm() / g0.norm()) < 1e-6
+
+
+def test_fp32_probe_computes_its_chains(wap):
+    """The roofline's FMA probe does the arithmetic it is credited with: each
+    thread's 8 chains a <- a x + y, summed, match a float64 evaluation."""
+    import ctypes
+    from wideanglepropagation_b200 import _lib
+    blocks, iters = 2, 64
+    out = torch.empty(blocks * 256, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib().wap_fp32_probe(blocks, iters, ctypes.c_void_p(out.data_ptr()),
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    x, y = np.float64(np.float32(0.999999)), np.float64(np.float32(1e-6))
+    a = (np.float64(np.float32(1e-3)) * np.arange(256)[:, None]).astype(np.float32).astype(np.float64) + np.arange(8)
+    for _ in range(iters):
+        a = a * x + y
+    ref = np.tile(a.sum(axis=1), blocks)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-5)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.lib().wap_fp32_probe(0, iters, ctypes.c_void_p(out.data_ptr()), None))

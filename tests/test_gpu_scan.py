@@ -116,3 +116,27 @@ def test_scan_rejects_unsupported(wap):
     classes[0].ny = classes[0].nx = 64
     with pytest.raises(ValueError, match="128, 256, 512 or 1024"):
         PersistentScan(classes)
+
+
+@pytest.mark.parametrize("n_slices,table", [(160, "hi"), (161, "full")])
+def test_twiddle_table_gate(wap, monkeypatch, n_slices, table):
+    """Scans of at most 160 slices run the hi-only stage-twiddle table, longer
+    ones hi + lo: the default run reproduces the forced table bit for bit on
+    each side of the gate, and both tables stay within 1e-5 of the FP64 oracle."""
+    from oracle import propagation_oracle as O
+    spec = [(128, n_slices, 3, 1)]
+    host = wap.synthetic.batched_scan_class(5, *spec[0])
+    H = O.angular_spectrum_propagation_kernel(host.ny, host.nx, (host.ps, host.ps), host.dz, host.energy)
+    p0 = O.move_probe(host.probe, tuple(host.positions[0]))
+    rex, _, _ = O.simulate_fresnel_as(host.potential[0], p0, H, host.dz, host.energy, return_wavefronts=False)
+    monkeypatch.delenv("WAP_SCHED_TW", raising=False)
+    ex_default, _, _ = _run(wap, _classes(wap, spec, seed=5), "persistent")
+    out = {}
+    for forced in ("hi", "full"):
+        monkeypatch.setenv("WAP_SCHED_TW", forced)
+        out[forced], _, _ = _run(wap, _classes(wap, spec, seed=5), "persistent")
+        assert O.rel_l2(out[forced][0][0].cpu().numpy(), rex) < 1e-5
+    monkeypatch.delenv("WAP_SCHED_TW")
+    assert torch.equal(ex_default[0], out[table][0])
+    other = "full" if table == "hi" else "hi"
+    assert not torch.equal(ex_default[0], out[other][0])

@@ -39,6 +39,7 @@ SIGNATURES = {
     "wap_gaussian_potential": (_I, [_I, _I, _I, _D, _D, _P, _P, _D, _D, _P, _P]),
     "wap_spectrum_propagate": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "wap_scan_grad_backward_ex": (_I, [_P, _P, _P, _P, _P]),
+    "wap_fp32_probe": (_I, [_I, _I, _P, _P]),
     "wap_line_transfer": (_I, [_I, _I, _P, _D, _D, _P, _P]),
     "wap_line_propagate": (_I, [_I, _I, _P, _P, _P, _I, _P, _P]),
     "wap_line_wpm": (_I, [_I, _I, _P, _P, _D, _P, _D, _P, _P]),

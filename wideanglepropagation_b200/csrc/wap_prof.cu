@@ -36,6 +36,24 @@ cudaEvent_t take() {
 
 bool prof_on() { return g_on; }
 
+// FP32 peak probe: every thread runs 8 independent FMA chains (a dependent
+// FMA's latency is covered by the other chains and the other warps), the
+// outer loop unrolled so that loop control is a few percent of the issue.
+__global__ void __launch_bounds__(256) fma_probe_kernel(int iters, float x, float y, float* out) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = 1e-3f * (float)threadIdx.x + (float)j;
+#pragma unroll 16
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = fmaf(a[j], x, y);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  out[(long long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -82,6 +100,15 @@ int wap_profile_reset(void) {
   }
   g_recs.clear();
   return WAP_OK;
+}
+
+int wap_fp32_probe(int blocks, int iters, float* out, void* stream) {
+  clear_error();
+  if (blocks < 1 || iters < 1 || !out) return fail(WAP_ERR_ARG, "need blocks >= 1, iters >= 1 and an output buffer");
+  count_launch();
+  fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, 0.999999f, 1e-6f, out);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? WAP_OK : cuda_fail(e, "fma_probe_kernel");
 }
 
 int wap_profile_read(int kind, long long* launches, double* total_ms, double* total_bytes) {
