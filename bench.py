@@ -466,7 +466,7 @@ def baseline_table():
             cpu = {m: cpu_rate(lambda m=m: O.simulate_fresnel_as(Vh[:cpu_slices], w.probe, Ho, w.dz, w.energy,
                                                                 mode=m, return_wavefronts=False), cpu_slices)
                    for m in ("fp64", "fp32")}
-        ms = timeit(gpu, 5 if kind != "wpm" else 2)
+        ms = timeit(gpu, 20 if kind == "fresnel" else 5 if kind == "as" else 2)
         ex, dp, _ = gpu()
         rows[name] = {
             "gpu_ms_per_call": ms, "gpu_slice_steps_per_s": w.n_slices / (ms / 1e3),

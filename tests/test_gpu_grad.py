@@ -195,3 +195,27 @@ def test_persistent_gradient_exit_wave_loss(wap, ckpt, dp_weight):
     L.backward()
     err = np.linalg.norm(V.grad.cpu().numpy() - Vr.grad.numpy()) / np.linalg.norm(Vr.grad.numpy())
     assert err < 5e-4, err
+
+
+@pytest.mark.parametrize("cfg", [(4, 4, 4), (4, 16, 2), (16, 4, 8)])
+def test_grad_small_element_shapes(wap, cfg):
+    """The adjoint on the 4-elements-per-thread pass shapes (row E, column E,
+    column width) that the one/two-probe launch shapes may use."""
+    from oracle import torch_oracle as T
+    from wideanglepropagation_b200 import _lib
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    Vt, V0, probe, pos, H, dz, E, target = _problem(N=5, seed=3)
+    L_ref, g_ref = T.loss_and_grad(V0, probe, H, dz, E, target, pos)
+    plan = wap.get_plan(64, 64, len(pos), _lib.WAP_OP_FRESNEL_AS)
+    old = plan.config()
+    try:
+        plan.set_config(*cfg)
+        V = torch.tensor(V0, dtype=torch.float32, device="cuda", requires_grad=True)
+        _, dp = simulate_fresnel_as_differentiable(V, probe, H, dz, E, positions=pos, ckpt_every=2)
+        L = ((dp - torch.tensor(target, device="cuda", dtype=torch.float32)) ** 2).sum()
+        L.backward()
+        assert plan.config() == cfg
+    finally:
+        plan.set_config(*old)
+    err = np.linalg.norm(V.grad.cpu().numpy() - g_ref) / np.linalg.norm(g_ref)
+    assert err < 1e-4, err

@@ -73,12 +73,12 @@ def store(ny, nx, op, n_bins, cfg, cls="any") -> None:
 def candidates(ny, nx):
     """Valid (row_e, col_e, col_w) launch shapes for an ny x nx grid."""
     out = []
-    for row_e in (8, 16):
+    for row_e in (4, 8, 16):
         if nx // row_e > 256 or nx < row_e:
             continue
-        for col_e in (8, 16):
+        for col_e in (4, 8, 16):
             T = ny // col_e
-            for col_w in (4, 8, 16, 32):
+            for col_w in (2, 4, 8, 16, 32):
                 if col_w > nx or col_w * T > 512 or ny * col_w * 8 > 160 * 1024:
                     continue
                 out.append((row_e, col_e, col_w))

@@ -181,6 +181,20 @@ static int occ_wpm_row_t(int rows, int K) {
     }                                                                   \
   } while (0)
 
+// the row and column passes also come with 4 elements per thread (grids up to
+// 1024): short per-thread chains for calls of one or two probes, whose few
+// CTAs per pass are latency-bound
+#define WAP_SIZE_CASES_E4(M) M(32, 4) M(64, 4) M(128, 4) M(256, 4) M(512, 4) M(1024, 4)
+#define WAP_DISPATCH_RC(FN, n, e)                                       \
+  do {                                                                  \
+    switch ((e) * 100000 + (n)) {                                       \
+      WAP_SIZE_CASES_E4(WAP_CASE_##FN)                                  \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 8)                                  \
+      WAP_SIZE_CASES(WAP_CASE_##FN, 16)                                 \
+      default: return cudaErrorInvalidValue;                            \
+    }                                                                   \
+  } while (0)
+
 #define WAP_CASE_row(N, E) case E * 100000 + N: return launch_row_t<N, E>(a, nb, k, st);
 #define WAP_CASE_col(N, E) case E * 100000 + N: return launch_col_t<N, E>(a, nb, k, st);
 #define WAP_CASE_wcol(N, E) case E * 100000 + N: return launch_wpm_col_t<N, E>(a, nb, k, st);
@@ -197,8 +211,8 @@ static int occ_wpm_row_t(int rows, int K) {
     }                                                                   \
   } while (0)
 
-cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(row, n, e); }
-cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(col, n, e); }
+cudaError_t launch_row(int n, int e, const RowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH_RC(row, n, e); }
+cudaError_t launch_col(int n, int e, const ColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH_RC(col, n, e); }
 cudaError_t launch_wpm_col(int n, int e, const WpmColArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wcol, n, e); }
 cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cudaStream_t st) { WAP_DISPATCH(wrow, n, e); }
 int wpm_col_occupancy(int n, int e, int k, int K) { WAP_DISPATCH_INT(wcolocc, n, e); }
@@ -289,7 +303,12 @@ static int default_col_w(int ny, int e, int nx) {
 }
 
 static bool config_valid(const wap_plan* p, int row_e, int col_e, int col_w) {
-  if ((row_e != 8 && row_e != 16) || (col_e != 8 && col_e != 16)) return false;
+  // 4 elements per thread: Fresnel/AS passes on grids up to 1024 (the WPM
+  // passes come with 8 and 16 only)
+  auto e_ok = [&](int e, int n) {
+    return e == 8 || e == 16 || (e == 4 && p->op == WAP_OP_FRESNEL_AS && n <= 1024);
+  };
+  if (!e_ok(row_e, p->nx) || !e_ok(col_e, p->ny)) return false;
   if (p->nx / row_e > kRowThreads) return false;
   if (col_w < 1 || (col_w & (col_w - 1)) || col_w > p->nx) return false;
   if (col_w * (p->ny / col_e) > kColThreads) return false;
