@@ -103,3 +103,20 @@ def test_atom_lists_reproduce_the_host_potentials():
     pos, rows = synthetic.batched_scan_class_atoms(3, 64, 5, 2, 2)
     V = np.stack([synthetic.gaussian_slice(64, 64, 0.05, pos[rows == r], 25.0, 0.25) for r in range(10)])
     assert np.allclose(V.reshape(2, 5, 64, 64) / 1.3575, w.potential, rtol=1e-6, atol=1e-6 * np.abs(V).max())
+
+
+def test_balanced_probe_groups():
+    """Probe groups split a batch evenly: 1024 probes at a nominal 111 make 9
+    groups of 114, 64 at 28 make 2 of 32; a batch below the size is one group."""
+    assert autotune.balanced_group(111, 1024) == 114
+    assert autotune.balanced_group(28, 64) == 32
+    assert autotune.balanced_group(444, 9) == 9
+    assert autotune.balanced_group(0, 100) == 0
+    for g in (7, 28, 111):
+        for B in (1, 9, 64, 100, 1024):
+            G = autotune.balanced_group(g, B)
+            ng = -(-B // G)
+            assert 1 <= G <= B
+            if B >= g:
+                assert g / 2 < G < 2 * g
+            assert G - ng <= B - (ng - 1) * G <= G   # the last group is within ng of the others

@@ -150,6 +150,17 @@ def default_scan_group(n: int) -> int:
     return max(1, -(-4 * 3 * sms // row_tiles))
 
 
+def balanced_group(group: int, batch: int) -> int:
+    """A probe-group size adjusted so that ``batch`` probes split into
+    round(batch / group) groups of equal size (a short last group would run
+    its dependency chain with most SMs idle); 0 stays 0 (the scheduler's own
+    rule, which balances the same way)."""
+    if group <= 0 or batch <= 0:
+        return group
+    ng = max(1, (batch + group // 2) // group)
+    return -(-batch // ng)
+
+
 def lookup_scan(n: int) -> int:
     """Cached probe-group size of the persistent scheduler for n x n grids (0: built-in)."""
     with _lock:

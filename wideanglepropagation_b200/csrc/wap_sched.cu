@@ -1312,6 +1312,10 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
       // available), and no more, so that the group's waves stay in L2: about
       // 4 x 444 tiles x 32 KB = 56 MB for every grid size on a 148-SM part
       G = std::max(1, (4 * s->grid + sc.row_tiles - 1) / sc.row_tiles);
+      // then even groups: the batch in round(B / G) groups of equal size, so
+      // that no small last group runs its chain with the SMs half idle
+      const int ng = std::max(1, (c.n_probes + G / 2) / G);
+      G = (c.n_probes + ng - 1) / ng;
     }
     G = std::min(G, c.n_probes);
     build_desc(steps, ci, c.n_probes, G, ticket, sc, desc);

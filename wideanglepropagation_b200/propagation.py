@@ -369,7 +369,7 @@ def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, gr
     D, N, n, _ = V.shape
     if group is None:
         from . import autotune
-        group = autotune.lookup_scan(n)
+        group = autotune.balanced_group(autotune.lookup_scan(n), exit_wave.shape[0])
     y0, x0, dny, dnx = det if det is not None else (0, 0, 0, 0)
     return _lib.ScanClass(n, N, D, exit_wave.shape[0], V.data_ptr(), dr.data_ptr() if dr is not None else None,
                           psi.data_ptr(), pos.data_ptr() if pos is not None else None, H.data_ptr(),

@@ -96,7 +96,8 @@ class PersistentScan:
     def __init__(self, classes: List[DeviceClass], groups: Optional[List[int]] = None):
         from . import autotune
         if groups is None:   # autotuned probe-group sizes (0: the scheduler's own)
-            groups = [autotune.lookup_scan(c.ny) if c.ny == c.nx else 0 for c in classes]
+            groups = [autotune.balanced_group(autotune.lookup_scan(c.ny), c.n_probes) if c.ny == c.nx else 0
+                      for c in classes]
         arr = (_lib.ScanClass * len(classes))()
         for i, c in enumerate(classes):
             if c.ny != c.nx:
