@@ -51,7 +51,9 @@ int wap_plan_create(wap_plan** plan, int ny, int nx, int max_batch, int op, int 
 int wap_plan_destroy(wap_plan* plan);
 
 /* FFT launch shape of the row pass (elements per thread) and column pass
- * (elements per thread, columns per CTA); set by the autotuner. */
+ * (elements per thread, columns per CTA); set by the autotuner.  Elements
+ * per thread: 8 or 16, and 4 for Fresnel/AS plans on grids up to 1024;
+ * WAP_ERR_ARG for a shape the kernels cannot launch. */
 int wap_plan_set_config(wap_plan* plan, int row_e, int col_e, int col_w);
 int wap_plan_get_config(const wap_plan* plan, int* row_e, int* col_e, int* col_w);
 
@@ -217,7 +219,9 @@ typedef struct wap_scan_class {
   double dz, energy;
   float* exit;               /* (n_probes, n, n) complex64: working buffer, exit waves */
   float* dp;                 /* (n_probes, n, n) float32, or (n_probes, det_ny, det_nx), or NULL */
-  int group;                 /* probes advanced together (0: automatic) */
+  int group;                 /* probes advanced together, used as given (0: automatic:
+                                about 4 x the resident CTAs in tiles, then evened out
+                                over n_probes) */
   int det_y0, det_x0;        /* detector window of dp (see wap_plan_set_detector); */
   int det_ny, det_nx;        /*   det_ny = det_nx = 0: the whole grid */
 } wap_scan_class;
