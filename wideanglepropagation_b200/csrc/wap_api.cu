@@ -528,6 +528,18 @@ cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t 
   return cudaSuccess;
 }
 
+// Whether a call tabulates exp(i phi(V)) (one elementwise kernel, bit for
+// bit the values the row pass would compute inline): when several probes see
+// each potential slice, and for one probe per draw while the table stays
+// within kSmallTransTable bytes of plan workspace - computed by a fully
+// occupied elementwise kernel it takes a long serial step out of the
+// latency-bound row pass of a single probe (512^2 x 100 slices: 2.07 -> 1.55 ms)
+constexpr size_t kSmallTransTable = size_t(1) << 30;
+static bool use_trans_table(const wap_plan* p, int n_probes, int n_slices, int n_draws) {
+  if (n_probes >= 2 * n_draws) return true;
+  return (size_t)n_draws * n_slices * p->ny * p->nx * sizeof(float2) <= kSmallTransTable;
+}
+
 // exp(i phi(V)) for every draw and slice into the plan's grow-only table
 int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st) {
   const size_t need = (size_t)n_draws * n_slices * p->ny * p->nx;
@@ -575,10 +587,10 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   r.src = reinterpret_cast<const float2*>(psi0);
   r.src_bstride = psi0_per_probe ? plane : 0;
   r.shifts = positions;
-  // When several probes see each potential slice, tabulate exp(i phi(V)) once
-  // per (draw, slice) instead of evaluating it per probe.
+  // exp(i phi(V)) tabulated once per (draw, slice) (use_trans_table), else
+  // evaluated inline by the row pass
   int trans_flag = ROW_TRANS;
-  if (n_probes >= 2 * n_draws && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) {
+  if (use_trans_table(p, n_probes, n_slices, n_draws) && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) {
     r.ttab = p->ttab;
     trans_flag = ROW_TRANS_TAB;
   } else {
@@ -696,7 +708,8 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
   // transmission shared by the probes of a draw, for the recompute and the
   // adjoint passes
   const float2* ttab = nullptr;
-  if (n_probes >= 2 * n_draws && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) ttab = p->ttab;
+  if (use_trans_table(p, n_probes, n_slices, n_draws) && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK)
+    ttab = p->ttab;
   else clear_error();
   r.psi = lam;
   r.psi_bstride = wstride;
