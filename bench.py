@@ -11,7 +11,8 @@ Printed JSON line (rank 0):
   e2e         the same through the public API (simulate_fresnel_as with
               positions/draws) from pinned host buffers, host<->device copies
               of the potential and of the diffraction patterns inside the
-              timed region
+              timed region (downloads on a second stream, overlapping the
+              next grid class's call)
   plain       slice-steps/s of the one-probe-per-launch path (same kernels)
   grad_over_fwd  t(forward + adjoint gradient) / t(forward) on the
               512^2, 64-slice, 64-probe inverse problem (checkpoint every 8)
@@ -768,6 +769,9 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None
     else:
         h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
     d2h = sum(o.numel() * 4 for *_, o in host)
+    # patterns go back on a second stream, so that a class's download overlaps
+    # the next class's multislice (the end of the timed region waits for it)
+    down = torch.cuda.Stream()
 
     def step():
         for i, (w, V, p, q, d, H, out) in enumerate(host):
@@ -777,7 +781,11 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None
                                            scale=1 / w.dz).view(D, N, w.ny, w.nx)
             _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False,
                                                max_angle=max_angle, sampling=(w.ps, w.ps))
-            out.copy_(dp, non_blocking=True)
+            down.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(down):
+                out.copy_(dp, non_blocking=True)
+            dp.record_stream(down)
+        torch.cuda.current_stream().wait_stream(down)
 
     for _ in range(max(1, args.warmup)):
         step()
