@@ -404,6 +404,24 @@ col_pass_kernel(const ColArgs a) {
   tile_store<NY>(ptile, tile, W, nx);
 }
 
+// exp(i phi) = (cos phi, sin phi) by the Taylor series of cos and sin in Horner
+// form, for |phi| <= 0.5 (truncation below 1e-10, under float rounding);
+// larger phases go to sincosf.  The WPM bin phases are small (dz |n_k - 1| k0).
+__device__ __forceinline__ float2 cis_small(float ph) {
+  if (fabsf(ph) > 0.5f) {
+    float s, c;
+    sincosf(ph, &s, &c);
+    return make_float2(c, s);
+  }
+  const float p2 = ph * ph;
+  // Taylor coefficients (-1)^j / (2j+1)! and (-1)^j / (2j)!
+  const float sn = ph * fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, 2.7557319e-06f, -1.9841270e-04f), 8.3333333e-03f),
+                                      -1.6666667e-01f), 1.0f);
+  const float cs = fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, -2.7557319e-07f, 2.4801587e-05f), -1.3888889e-03f),
+                                           4.1666667e-02f), -0.5f), 1.0f);
+  return make_float2(cs, sn);
+}
+
 // ----------------------------------------------------------------------------
 // WPM (propagation.py:215-256)
 // ----------------------------------------------------------------------------
@@ -546,9 +564,18 @@ wpm_col_kernel(const WpmColArgs a) {
     q0[e] = a.k02 - (__ldg(a.ky2 + ky) + kx2);
     v[e] = cmul_hl(v[e], __ldg(a.hvac + (long long)ky * nx + col), __ldg(a.hvac_lo + (long long)ky * nx + col));
   }
-  float sq0[E];
+  // Bin phase dz a_k / (sqrt(q0 + a_k) + sqrt(q0)) = (dz a_k / (2 sqrt(q0))) f(a_k / q0)
+  // with f(x) = 2 / (1 + sqrt(1 + x)) = 1 - x/4 + x^2/8 - 5 x^3/64 + O(x^4): to
+  // float rounding while |a_k| <= q0 / 128 (the x^4 term is below 1e-9), which
+  // holds away from the evanescent edge (|a_k| / k0^2 is 2|n_k - 1|, ~1e-4).
+  // pa = dz / (2 sqrt(q0)) (0 when q0 <= 0), pr = 1 / q0; other elements take
+  // the direct formulas below.
+  float pa[E], pr[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) sq0[e] = sqrtf(fabsf(q0[e]));
+  for (int e = 0; e < E; ++e) {
+    pr[e] = 1.0f / q0[e];
+    pa[e] = q0[e] > 0.0f ? 0.5f * a.dz * sqrtf(pr[e]) : 0.0f;
+  }
 
   float2* ftile = a.fields + (long long)b * a.K * plane + (long long)blockIdx.x * W;
   const int kb = blockIdx.z * a.kpg, ke = min(kb + a.kpg, a.K);
@@ -558,15 +585,23 @@ wpm_col_kernel(const WpmColArgs a) {
     float2 u[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const float qk = q0[e] + ak;
+      const float x = ak * pr[e];
+      if (pa[e] > 0.0f && fabsf(x) <= 0.0078125f) {
+        const float ph = ak * pa[e] * fmaf(x, fmaf(x, fmaf(x, -0.078125f, 0.125f), -0.25f), 1.0f);
+        u[e] = cmul(v[e], cis_small(ph));
+        continue;
+      }
+      const float q0e = 1.0f / pr[e];
+      const float sq0 = sqrtf(fabsf(q0e));
+      const float qk = q0e + ak;
       float2 h;
-      if (q0[e] >= 0.0f && qk >= 0.0f) {
+      if (q0e >= 0.0f && qk >= 0.0f) {
         float s, cc;
-        sincosf(a.dz * ak / (sqrtf(qk) + sq0[e]), &s, &cc);
+        sincosf(a.dz * ak / (sqrtf(qk) + sq0), &s, &cc);
         h = make_float2(cc, s);
         u[e] = cmul(v[e], h);
-      } else if (q0[e] < 0.0f && qk < 0.0f) {
-        const float g = expf(a.dz * ak / (sqrtf(-qk) + sq0[e]));
+      } else if (q0e < 0.0f && qk < 0.0f) {
+        const float g = expf(a.dz * ak / (sqrtf(-qk) + sq0));
         u[e] = cscale(v[e], g);
       } else {
         // one side evanescent: exact H_k; undo the vacuum factor on X
@@ -582,8 +617,8 @@ wpm_col_kernel(const WpmColArgs a) {
         // v = X * hv; want X * hk.  |hv| is 1 (propagating vacuum) or a
         // decay factor; divide it out explicitly.
         const float n2 = fmaf(hv.x, hv.x, hv.y * hv.y);
-        const float2 x = n2 > 0.0f ? cscale(cmulc(v[e], hv), 1.0f / n2) : make_float2(0.f, 0.f);
-        u[e] = cmul(x, hk);
+        const float2 x2 = n2 > 0.0f ? cscale(cmulc(v[e], hv), 1.0f / n2) : make_float2(0.f, 0.f);
+        u[e] = cmul(x2, hk);
       }
     }
     fft<NY, E, true>(u, t, xs, tw);
