@@ -95,14 +95,33 @@ size_t col_smem_bytes(int w, int extra_bytes) {
   return (size_t)N * w * sizeof(float2) + FFTPlan<N, E>::TW_SIZE * sizeof(float4) + extra_bytes;
 }
 
+// Row and column passes go out with programmatic dependent launch (the
+// kernels wait for their predecessor first thing): in a chain of short,
+// latency-bound passes the next pass is already resident when one finishes
+// (C1 0.26 -> 0.19 ms per call).  The WPM passes launch normally: their large
+// CTAs parked early cost more than the launch latency saved (C3 12.5 vs 13.1 ms).
+template <class K, class A>
+static cudaError_t launch_pdl(K kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const A& args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args);
+}
+
 template <int N, int E>
 static cudaError_t launch_row_t(const RowArgs& a, int nb, int rows, cudaStream_t st) {
   const size_t smem = row_smem_bytes<N, E>(rows, 0);
   cudaError_t err = prep_smem(row_pass_kernel<N, E>, smem);
   if (err != cudaSuccess) return err;
   count_launch();
-  row_pass_kernel<N, E><<<dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(row_pass_kernel<N, E>, dim3(a.ny / rows, nb), rows * FFTPlan<N, E>::T, smem, st, a);
 }
 
 template <int N, int E>
@@ -114,12 +133,10 @@ static cudaError_t launch_col_t(const ColArgs& a, int nb, int w, cudaStream_t st
   count_launch();
   if (a.flags & COL_SEED) {
     if ((err = prep_smem(col_pass_kernel<N, E, true>, smem)) != cudaSuccess) return err;
-    col_pass_kernel<N, E, true><<<grid, threads, smem, st>>>(a);
-  } else {
-    if ((err = prep_smem(col_pass_kernel<N, E, false>, smem)) != cudaSuccess) return err;
-    col_pass_kernel<N, E, false><<<grid, threads, smem, st>>>(a);
+    return launch_pdl(col_pass_kernel<N, E, true>, grid, threads, smem, st, a);
   }
-  return cudaGetLastError();
+  if ((err = prep_smem(col_pass_kernel<N, E, false>, smem)) != cudaSuccess) return err;
+  return launch_pdl(col_pass_kernel<N, E, false>, grid, threads, smem, st, a);
 }
 
 template <int N, int E>

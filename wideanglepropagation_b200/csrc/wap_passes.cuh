@@ -151,6 +151,17 @@ static __global__ void __launch_bounds__(256) interleave_h_kernel(const float2* 
   }
 }
 
+// Programmatic dependent launch of the row and column passes: a pass launched
+// with the attribute may become resident while the previous kernel in the
+// stream drains; griddepcontrol.wait then blocks until that kernel has
+// completed and its writes are visible (a no-op for a normal launch), and
+// launch_dependents lets the next pass start the same way.  Both come first
+// in the kernel, before any global read.
+__device__ __forceinline__ void pdl_wait_then_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ----------------------------------------------------------------------------
 // row pass
 // ----------------------------------------------------------------------------
@@ -171,6 +182,7 @@ row_pass_kernel(const RowArgs a) {
   extern __shared__ float4 smem_raw[];
   float4* tw = smem_raw;
   float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
+  pdl_wait_then_release();
   for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
@@ -310,6 +322,7 @@ col_pass_kernel(const ColArgs a) {
   extern __shared__ float4 smem_raw[];
   float4* tw = smem_raw;
   float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
+  pdl_wait_then_release();
   for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
