@@ -266,3 +266,17 @@ def test_pinned_host_inputs_upload_on_a_side_stream(wap):
                                             draw=torch.from_numpy(w.draw_of_probe).pin_memory(),
                                             return_wavefronts=False)
         assert torch.equal(ex, ref_ex) and torch.equal(dp, ref_dp)
+
+
+def test_wpm_strong_phase(wap):
+    """A strong potential in thick slices: bin phases well above 0.5 rad, so the
+    column pass's exp(i phi) takes its sincosf branch next to the Taylor one."""
+    from oracle import propagation_oracle as O
+    rng = np.random.default_rng(12)
+    n, ps, dz, E = 64, 0.05, 5.0, 300e3
+    V = rng.uniform(0, 2000, (3, n, n)).astype(np.float32)
+    psi = (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))).astype(np.complex64)
+    ex, dp, _ = wap.simulate_wpm(V, psi, dz, E, (ps, ps), 8, 1.0)
+    rex, rdp, _ = O.simulate_wpm(V, psi, dz, E, (ps, ps), 8, 1.0)
+    assert rel(np_(ex), rex) < TOL
+    assert rel(np_(dp), rdp) < TOL
