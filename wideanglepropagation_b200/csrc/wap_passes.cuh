@@ -417,15 +417,47 @@ col_pass_kernel(const ColArgs a) {
   tile_store<NY>(ptile, tile, W, nx);
 }
 
+// The WPM bin propagator applied to v = X * Hvac by the direct formulas, for
+// the pixels outside the series' range (near or beyond the evanescent edge).
+// Rarely taken, so kept out of line: the unrolled bin loop stays small.
+static __device__ __noinline__ float2 wpm_bin_direct(float2 v, float pr, float ak, float dz, const float2* hvac) {
+  const float q0 = 1.0f / pr;
+  const float sq0 = sqrtf(fabsf(q0));
+  const float qk = q0 + ak;
+  if (q0 >= 0.0f && qk >= 0.0f) {
+    float s, c;
+    sincosf(dz * ak / (sqrtf(qk) + sq0), &s, &c);
+    return cmul(v, make_float2(c, s));
+  }
+  if (q0 < 0.0f && qk < 0.0f) return cscale(v, expf(dz * ak / (sqrtf(-qk) + sq0)));
+  // one side evanescent: exact H_k; undo the vacuum factor on X.  v = X * hv;
+  // |hv| is 1 (propagating vacuum) or a decay factor: divide it out explicitly
+  const float2 hv = __ldg(hvac);
+  float2 hk;
+  if (qk >= 0.0f) {
+    float s, c;
+    sincosf(dz * sqrtf(qk), &s, &c);
+    hk = make_float2(c, s);
+  } else {
+    hk = make_float2(expf(-dz * sqrtf(-qk)), 0.0f);
+  }
+  const float n2 = fmaf(hv.x, hv.x, hv.y * hv.y);
+  const float2 x = n2 > 0.0f ? cscale(cmulc(v, hv), 1.0f / n2) : make_float2(0.f, 0.f);
+  return cmul(x, hk);
+}
+
+// exp(i phi) for phases beyond the Taylor range, out of line for the same reason
+static __device__ __noinline__ float2 cis_large(float ph) {
+  float s, c;
+  sincosf(ph, &s, &c);
+  return make_float2(c, s);
+}
+
 // exp(i phi) = (cos phi, sin phi) by the Taylor series of cos and sin in Horner
 // form, for |phi| <= 0.5 (truncation below 1e-10, under float rounding);
 // larger phases go to sincosf.  The WPM bin phases are small (dz |n_k - 1| k0).
 __device__ __forceinline__ float2 cis_small(float ph) {
-  if (fabsf(ph) > 0.5f) {
-    float s, c;
-    sincosf(ph, &s, &c);
-    return make_float2(c, s);
-  }
+  if (fabsf(ph) > 0.5f) return cis_large(ph);
   const float p2 = ph * ph;
   // Taylor coefficients (-1)^j / (2j+1)! and (-1)^j / (2j)!
   const float sn = ph * fmaf(p2, fmaf(p2, fmaf(p2, fmaf(p2, 2.7557319e-06f, -1.9841270e-04f), 8.3333333e-03f),
@@ -604,35 +636,7 @@ wpm_col_kernel(const WpmColArgs a) {
         u[e] = cmul(v[e], cis_small(ph));
         continue;
       }
-      const float q0e = 1.0f / pr[e];
-      const float sq0 = sqrtf(fabsf(q0e));
-      const float qk = q0e + ak;
-      float2 h;
-      if (q0e >= 0.0f && qk >= 0.0f) {
-        float s, cc;
-        sincosf(a.dz * ak / (sqrtf(qk) + sq0), &s, &cc);
-        h = make_float2(cc, s);
-        u[e] = cmul(v[e], h);
-      } else if (q0e < 0.0f && qk < 0.0f) {
-        const float g = expf(a.dz * ak / (sqrtf(-qk) + sq0));
-        u[e] = cscale(v[e], g);
-      } else {
-        // one side evanescent: exact H_k; undo the vacuum factor on X
-        const float2 hv = __ldg(a.hvac + (long long)(t + T * e) * nx + col);
-        float2 hk;
-        if (qk >= 0.0f) {
-          float s, cc;
-          sincosf(a.dz * sqrtf(qk), &s, &cc);
-          hk = make_float2(cc, s);
-        } else {
-          hk = make_float2(expf(-a.dz * sqrtf(-qk)), 0.0f);
-        }
-        // v = X * hv; want X * hk.  |hv| is 1 (propagating vacuum) or a
-        // decay factor; divide it out explicitly.
-        const float n2 = fmaf(hv.x, hv.x, hv.y * hv.y);
-        const float2 x2 = n2 > 0.0f ? cscale(cmulc(v[e], hv), 1.0f / n2) : make_float2(0.f, 0.f);
-        u[e] = cmul(x2, hk);
-      }
+      u[e] = wpm_bin_direct(v[e], pr[e], ak, a.dz, a.hvac + (long long)(t + T * e) * nx + col);
     }
     fft<NY, E, true>(u, t, xs, tw);
     __syncthreads();
