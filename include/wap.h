@@ -262,6 +262,7 @@ int wap_scan_grad_backward_ex(wap_scan* scan, const float* grad_dp, const float*
  * else is allocated). */
 int wap_scan_bind(wap_scan* scan, int n_classes, const wap_scan_class* classes);
 int wap_scan_status(wap_scan* scan, int* status);
+/* Work-queue tickets, launched CTAs and the probe-group size class 0 runs with. */
 int wap_scan_info(const wap_scan* scan, long long* tickets, int* grid, int* group0);
 int wap_scan_destroy(wap_scan* scan);
 /* Failure injection for tests (no counterpart in the reference): tiles of

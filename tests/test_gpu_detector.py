@@ -115,3 +115,33 @@ def test_bad_window_rejected(wap):
     with pytest.raises(ValueError):
         _lib.check(_lib.lib().wap_plan_set_detector(plan.handle, -1, 0, 10, 10))
     _lib.check(_lib.lib().wap_plan_set_detector(plan.handle, 0, 0, 0, 0))
+
+
+@pytest.mark.parametrize("n_side", [2, 3])   # 4 probes: pass kernels; 9: persistent scheduler
+def test_gradient_window_and_exit_loss(wap, n_side):
+    """A loss on the cropped pattern and on the exit wave together: the seed
+    scatters the window's dL/d(dp) and adds fft2(dL/d(exit) / 2); the result
+    equals the full-grid pattern cropped by hand."""
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    V, probe, pos, ps, dz, E = _case(n=128, N=6, n_side=n_side, seed=2)
+    n = V.shape[-1]
+    H = wap.fresnel_propagation_kernel(n, n, (ps, ps), dz, E)
+    dev = torch.device("cuda")
+    y0, x0, wy, wx = wap.detector_window((n, n), (ps, ps), E, 45.0)
+    rng = np.random.default_rng(8)
+    target = torch.tensor(rng.random((len(pos), wy, wx)), dtype=torch.float32, device=dev)
+    c = torch.tensor(rng.normal(size=(len(pos), n, n)) + 1j * rng.normal(size=(len(pos), n, n)),
+                     dtype=torch.complex64, device=dev)
+    Vt = torch.tensor(V, device=dev)
+
+    V1 = Vt.clone().requires_grad_(True)
+    ex1, dpc = simulate_fresnel_as_differentiable(V1, probe, H, dz, E, positions=pos, ckpt_every=2, max_angle=45.0,
+                                                  sampling=ps)
+    (((dpc - target) ** 2).sum() + 1e-2 * (ex1 * c).real.sum()).backward()
+
+    V2 = Vt.clone().requires_grad_(True)
+    ex2, dpf = simulate_fresnel_as_differentiable(V2, probe, H, dz, E, positions=pos, ckpt_every=2)
+    (((dpf[..., y0:y0 + wy, x0:x0 + wx] - target) ** 2).sum() + 1e-2 * (ex2 * c).real.sum()).backward()
+
+    rel = float((V1.grad - V2.grad).norm() / V2.grad.norm())
+    assert rel < 1e-6, rel

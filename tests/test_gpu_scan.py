@@ -140,3 +140,18 @@ def test_twiddle_table_gate(wap, monkeypatch, n_slices, table):
     assert torch.equal(ex_default[0], out[table][0])
     other = "full" if table == "hi" else "hi"
     assert not torch.equal(ex_default[0], out[other][0])
+
+
+def test_automatic_groups_are_balanced(wap):
+    """With group 0 the library picks about 4 x the resident CTAs in tiles and
+    evens it out over the batch: 64 probes on 512^2 (nominal 28 on 148 SMs)
+    run as two groups of 32."""
+    from wideanglepropagation_b200.scan import PersistentScan
+    classes = _classes(wap, [(512, 2, 8, 1)])
+    assert classes[0].n_probes == 64
+    info = PersistentScan(classes, [0]).info()
+    nominal = -(-4 * info["grid"] // (512 * 512 // 4096))
+    ng = max(1, (64 + nominal // 2) // nominal)
+    assert info["group0"] == -(-64 // ng)
+    if info["grid"] == 444:
+        assert info["group0"] == 32

@@ -1021,6 +1021,7 @@ struct wap_scan {
   std::vector<size_t> ttab_elems;
   std::vector<wap_scan_class> cls;
   std::vector<Physics> phys;
+  std::vector<int> groups;          // per class: probes advanced together
 };
 
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -1236,6 +1237,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   if (!encode) return fail(WAP_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   cudaGetDevice(&s->device);
   s->n_classes = n_classes;
+  s->groups.clear();
   s->cls.assign(classes, classes + n_classes);
   s->grad = ckpt_every > 0;
   s->ckpt_every = ckpt_every;
@@ -1453,6 +1455,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
       G = (c.n_probes + ng - 1) / ng;
     }
     G = std::min(G, c.n_probes);
+    s->groups.push_back(G);
     build_desc(steps, ci, c.n_probes, G, ticket, sc, desc);
     if (s->grad) build_desc(steps_bwd, ci, c.n_probes, G, ticket_bwd, sc, desc_bwd);
     step_off.push_back(steps_all.size());
@@ -1737,7 +1740,7 @@ int wap_scan_info(const wap_scan* s, long long* tickets, int* grid, int* group0)
   if (!s || !tickets || !grid || !group0) return fail(WAP_ERR_ARG, "NULL argument");
   *tickets = s->n_tickets;
   *grid = s->grid;
-  *group0 = 0;
+  *group0 = s->groups.empty() ? 0 : s->groups[0];
   return WAP_OK;
 }
 

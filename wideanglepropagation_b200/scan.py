@@ -124,7 +124,7 @@ class PersistentScan:
     def info(self) -> dict:
         t, g, g0 = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
         _lib.check(_lib.lib().wap_scan_info(self.handle, ctypes.byref(t), ctypes.byref(g), ctypes.byref(g0)))
-        return {"tickets": t.value, "grid": g.value}
+        return {"tickets": t.value, "grid": g.value, "group0": g0.value}
 
     def debug_stall(self, pass_index: int, spin_limit: int = 0) -> None:
         _lib.check(_lib.lib().wap_scan_debug_stall(self.handle, int(pass_index), int(spin_limit)))
