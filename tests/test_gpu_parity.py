@@ -280,3 +280,33 @@ def test_wpm_strong_phase(wap):
     rex, rdp, _ = O.simulate_wpm(V, psi, dz, E, (ps, ps), 8, 1.0)
     assert rel(np_(ex), rex) < TOL
     assert rel(np_(dp), rdp) < TOL
+
+
+@pytest.mark.parametrize("ny,nx", [(64, 64), (1024, 1024), (128, 512)])
+def test_every_launch_shape_other_grids(wap, ny, nx):
+    """Every launch shape the autotuner may pick (4, 8 or 16 elements per
+    thread, 2 to 32 columns per column CTA), on a small, a large and a
+    non-square grid, against the oracle."""
+    from wideanglepropagation_b200 import autotune, _lib
+    from oracle import propagation_oracle as O
+    rng = np.random.default_rng(13)
+    V = rng.uniform(0, 30, (2, ny, nx)).astype(np.float32)
+    psi = (rng.normal(size=(ny, nx)) + 1j * rng.normal(size=(ny, nx))).astype(np.complex64)
+    H = O.angular_spectrum_propagation_kernel(ny, nx, (0.05, 0.05), 2.0, 300e3)
+    rex, rdp, _ = O.simulate_fresnel_as(V, psi, H, 2.0, 300e3, return_wavefronts=False)
+    plan = wap.get_plan(ny, nx, 1, _lib.WAP_OP_FRESNEL_AS)
+    old = plan.config()
+    tried = 0
+    try:
+        for cfg in autotune.candidates(ny, nx):
+            try:
+                plan.set_config(*cfg)
+            except ValueError:
+                continue   # a shape the kernels cannot launch on this grid
+            ex, dp, _ = wap.simulate_fresnel_as(V, psi, H, 2.0, 300e3, return_wavefronts=False)
+            assert rel(np_(ex), rex) < TOL, cfg
+            assert rel(np_(dp), rdp) < TOL, cfg
+            tried += 1
+    finally:
+        plan.set_config(*old)
+    assert tried > 0
