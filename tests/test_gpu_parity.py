@@ -310,3 +310,33 @@ def test_every_launch_shape_other_grids(wap, ny, nx):
     finally:
         plan.set_config(*old)
     assert tried > 0
+
+
+def test_every_wpm_launch_shape(wap):
+    """The WPM passes at every launch shape a WPM plan accepts (8 or 16
+    elements per thread, 2 to 32 columns per column CTA) against the oracle."""
+    from wideanglepropagation_b200 import autotune, _lib
+    from oracle import propagation_oracle as O
+    n, K = 128, 8
+    rng = np.random.default_rng(14)
+    V = rng.uniform(0, 60, (3, n, n)).astype(np.float32)
+    psi = (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))).astype(np.complex64)
+    rex, rdp, _ = O.simulate_wpm(V, psi, 2.0, 300e3, (0.05, 0.05), K, 1.0, return_wavefronts=False)
+    plan = wap.get_plan(n, n, 1, _lib.WAP_OP_WPM, K)
+    old = plan.config()
+    with pytest.raises(ValueError):
+        plan.set_config(4, 8, 8)
+    tried = 0
+    try:
+        for cfg in autotune.candidates(n, n):
+            try:
+                plan.set_config(*cfg)
+            except ValueError:
+                continue   # 4 elements per thread: Fresnel/AS plans only
+            ex, dp, _ = wap.simulate_wpm(V, psi, 2.0, 300e3, (0.05, 0.05), K, 1.0, return_wavefronts=False)
+            assert rel(np_(ex), rex) < TOL, cfg
+            assert rel(np_(dp), rdp) < TOL, cfg
+            tried += 1
+    finally:
+        plan.set_config(*old)
+    assert tried > 0
