@@ -219,3 +219,28 @@ def test_grad_small_element_shapes(wap, cfg):
         plan.set_config(*old)
     err = np.linalg.norm(V.grad.cpu().numpy() - g_ref) / np.linalg.norm(g_ref)
     assert err < 1e-4, err
+
+
+def test_grad_non_square_grid(wap):
+    """The pass-kernel adjoint on a 64 x 128 grid (the persistent scheduler
+    takes square grids only) against the autograd of the torch restatement."""
+    import wideanglepropagation_b200.synthetic as S
+    from oracle import propagation_oracle as O
+    from oracle import torch_oracle as T
+    from wideanglepropagation_b200.autograd import simulate_fresnel_as_differentiable
+    rng = np.random.default_rng(21)
+    ny, nx, N, ps, dz, E = 64, 128, 5, 0.1, 2.0, 300e3
+    Vt = S.random_gaussian_stack(rng, N, ny, nx, ps, 4, 20.0, 0.3) / dz
+    V0 = 0.5 * S.random_gaussian_stack(rng, N, ny, nx, ps, 4, 20.0, 0.3) / dz
+    probe = S.aperture_probe(ny, nx, ps, E, 25.0, -50.0, dtype=np.complex64)
+    pos = np.array([[20, 40], [32, 64], [50, 100]], dtype=np.int32)
+    H = O.fresnel_propagation_kernel(ny, nx, (ps, ps), dz, E)
+    _, target = T.simulate(torch.tensor(Vt), probe, H, dz, E, pos)
+    L_ref, g_ref = T.loss_and_grad(V0, probe, H, dz, E, target.numpy(), pos)
+    V = torch.tensor(V0, dtype=torch.float32, device="cuda", requires_grad=True)
+    _, dp = simulate_fresnel_as_differentiable(V, probe, H, dz, E, positions=pos, ckpt_every=2)
+    L = ((dp - torch.tensor(target.numpy(), device="cuda", dtype=torch.float32)) ** 2).sum()
+    L.backward()
+    assert abs(float(L) - L_ref) / L_ref < 1e-4
+    err = np.linalg.norm(V.grad.cpu().numpy() - g_ref) / np.linalg.norm(g_ref)
+    assert err < 1e-4, err
