@@ -61,6 +61,8 @@ def parse():
                          "persistent scheduler")
     ap.add_argument("--profile-wpm", action="store_true",
                     help="WPM case for ncu captures: C3 (512^2, K=16, plane wave) at 3 slices, two calls")
+    ap.add_argument("--profile-single", action="store_true",
+                    help="single-probe case for ncu captures: C2 (1024^2 AS, plane wave) at 10 slices, two calls")
     ap.add_argument("--table", action="store_true",
                     help="per-configuration table (C1 Fresnel 256^2, C2 AS 1024^2, C3 WPM 512^2; one probe): B200 "
                          "time, CPU FP64/FP32 restatement on a bounded sample, error vs the FP64 oracle at full "
@@ -200,6 +202,9 @@ def main():
         return
     if args.profile_wpm:
         profile_wpm()
+        return
+    if args.profile_single:
+        profile_single()
         return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
@@ -409,6 +414,20 @@ def profile_wpm():
         wap.simulate_wpm(V, pr, w.dz, w.energy, (w.ps, w.ps), w.n_bins, w.power_spacing, return_wavefronts=False)
     torch.cuda.synchronize()
     print(json.dumps({"profile_wpm": "ok"}))
+
+
+def profile_single():
+    import torch
+    import wideanglepropagation_b200 as wap
+    w = wap.synthetic.angular_spectrum_diamond(0, n_slices=10)
+    dev = torch.device("cuda", 0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    for _ in range(2):
+        wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_single": "ok"}))
 
 
 def baseline_table():
