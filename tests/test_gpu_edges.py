@@ -122,3 +122,22 @@ def test_fp32_probe_computes_its_chains(wap):
     np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-5)
     with pytest.raises(ValueError):
         _lib.check(_lib.lib().wap_fp32_probe(0, iters, ctypes.c_void_p(out.data_ptr()), None))
+
+
+def test_transfer_split_cache_follows_changes(wap):
+    """A complex128 transfer function on the device is split into hi + lo once
+    and reused; an in-place change of it must not reuse the stale split."""
+    rng = np.random.default_rng(5)
+    n = 64
+    V = torch.tensor(rng.uniform(0, 30, (3, n, n)).astype(np.float32), device="cuda")
+    psi = torch.tensor((rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))).astype(np.complex64), device="cuda")
+    H = wap.angular_spectrum_propagation_kernel(n, n, (0.05, 0.05), 2.0, 300e3)
+    assert H.dtype == torch.complex128 and H.is_cuda
+    e1, _, _ = wap.simulate_fresnel_as(V, psi, H, 2.0, 300e3, return_wavefronts=False)
+    e2, _, _ = wap.simulate_fresnel_as(V, psi, H, 2.0, 300e3, return_wavefronts=False)
+    assert torch.equal(e1, e2)
+    H.mul_(torch.exp(1j * torch.linspace(0, 1, n * n, dtype=torch.float64, device="cuda")).reshape(n, n))
+    e3, _, _ = wap.simulate_fresnel_as(V, psi, H, 2.0, 300e3, return_wavefronts=False)
+    e4, _, _ = wap.simulate_fresnel_as(V, psi, H.clone(), 2.0, 300e3, return_wavefronts=False)
+    assert torch.equal(e3, e4)
+    assert not torch.equal(e1, e3)

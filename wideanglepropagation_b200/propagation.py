@@ -93,19 +93,42 @@ def _to(x, dtype, device) -> torch.Tensor:
     return x.to(device=device, dtype=dtype).contiguous()
 
 
+# Recent splits of complex128 device tensors: (source tensor, its version,
+# device, hi, lo).  An entry keeps its source alive, so no other tensor can
+# take its memory while cached, and an in-place change of the source bumps
+# its version and misses.
+_SPLIT_CACHE_MAX = 4
+_split_cache: list = []
+_split_lock = threading.Lock()
+
+
 def split_transfer(H, device):
     """complex64 hi part and remainder of a transfer function.
 
     A complex128 H is split into H_hi = (complex64)H and H_lo = H - H_hi; the
     kernels apply X*H_hi + X*H_lo, which removes the rounding of H that would
     otherwise repeat identically at every slice.  A complex64 H has no lo part.
+    A complex128 tensor already on the device is split once and reused while
+    it is unchanged (a transfer function normally serves many calls).
     """
     t = H if isinstance(H, torch.Tensor) else torch.as_tensor(np.asarray(H))
     if t.dtype == torch.complex128:
+        dev = torch.device(device)
+        cacheable = t.device.type == "cuda" and t.device == dev
+        if cacheable:
+            with _split_lock:
+                for i, (src, ver, d, hi, lo) in enumerate(_split_cache):
+                    if src is t and ver == t._version and d == dev:
+                        _split_cache.append(_split_cache.pop(i))
+                        return hi, lo
         t = t.to(device)
-        hi = t.to(torch.complex64)
-        lo = (t - hi.to(torch.complex128)).to(torch.complex64)
-        return hi.contiguous(), lo.contiguous()
+        hi = t.to(torch.complex64).contiguous()
+        lo = (t - hi.to(torch.complex128)).to(torch.complex64).contiguous()
+        if cacheable:
+            with _split_lock:
+                _split_cache.append((H, H._version, dev, hi, lo))
+                del _split_cache[:-_SPLIT_CACHE_MAX]
+        return hi, lo
     return _to(t, torch.complex64, device), None
 
 
@@ -402,8 +425,11 @@ def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None):
 def release_caches() -> None:
     """Free the device memory the library keeps between calls: cached plans
     (twiddles, WPM workspaces), cached forward scans (transmission tables,
-    interleaved propagators) and idle pooled gradient scans."""
+    interleaved propagators), idle pooled gradient scans and cached splits of
+    complex128 transfer functions."""
     torch.cuda.synchronize()
+    with _split_lock:
+        _split_cache.clear()
     with _scans_lock:
         for h in _scans.values():
             _lib.lib().wap_scan_destroy(h)
