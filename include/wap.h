@@ -152,6 +152,31 @@ int wap_wpm_naive_step(int ny, int nx, const double* wave, const double* n_map, 
 int wap_gaussian_potential(int n_slices, int ny, int nx, double ps_y, double ps_x, const double* atoms,
                            const int32_t* slice_start, double sigma, double scale, float* V, void* stream);
 
+/* Convergent probe on the device, into out ((ny, nx) complex64 of the plan's
+ * grid): a hard aperture |f| lambda < alpha_mrad / 1000 with the defocus phase
+ * exp(-i pi lambda defocus |f|^2) inside it (f from fftfreq(ny, ps_y) x
+ * fftfreq(nx, ps_x), float64), inverse-transformed, normalised to
+ * sum |psi|^2 = ny nx and, with centred != 0, rolled to the grid centre
+ * (ny/2, nx/2) - the position move_probe (propagation.py:263-276) measures
+ * shifts from.  Replaces the host-side probe construction that precedes the
+ * multislice (the reference's notebooks build probes with abTEM on the host,
+ * e.g. wpm/cbed.ipynb; the benchmark configurations use this probe model).
+ * The plan keeps one 8-byte counter, allocated on the first call. */
+int wap_aperture_probe(wap_plan* plan, double ps_y, double ps_x, double energy, double alpha_mrad, double defocus,
+                       int centred, float* out, void* stream);
+
+/* Sum diffraction patterns per output pattern, in a fixed order (no atomics):
+ *   out[p] = sum_{j = start[p]}^{start[p+1]-1} dp[probes[j]]
+ * dp is (n_probes, plane) float32, out (n_patterns, plane), start
+ * (n_patterns + 1) and probes int32, all device pointers.  With several
+ * frozen-phonon draws per scan position (probes of one position sharing a
+ * pattern) this is the per-position accumulation of the incoherent average
+ * the reference's callers form by summing simulate_fresnel_as patterns over
+ * configurations.  Indices outside [0, n_probes) are skipped and set *bad = 1
+ * (bad: device int, nullable). */
+int wap_pattern_accumulate(const float* dp, int n_probes, long long plane, const int32_t* start,
+                           const int32_t* probes, int n_patterns, float* out, int* bad, void* stream);
+
 /* WPM adaptive-binning multislice forward, propagation.py:358-387 with the
  * step of propagation.py:215-256 (n_bins reference indices spaced
  * n_min + (n_max - n_min) t^power_spacing per slice, smoothstep blend of the
@@ -262,6 +287,12 @@ int wap_scan_grad_backward_ex(wap_scan* scan, const float* grad_dp, const float*
  * else is allocated). */
 int wap_scan_bind(wap_scan* scan, int n_classes, const wap_scan_class* classes);
 int wap_scan_status(wap_scan* scan, int* status);
+/* Non-blocking form: enqueue on `stream` a copy of the scan's status word (0
+ * or WAP_ERR_TIMEOUT, as left by the last run issued before it on that
+ * stream) into host_status, a host int the GPU can write (pinned memory).
+ * The value is valid once the stream has reached the copy.  The Python layer
+ * turns a non-zero status into WapError. */
+int wap_scan_status_async(wap_scan* scan, int* host_status, void* stream);
 /* Work-queue tickets, launched CTAs and the probe-group size class 0 runs with. */
 int wap_scan_info(const wap_scan* scan, long long* tickets, int* grid, int* group0);
 int wap_scan_destroy(wap_scan* scan);
@@ -275,6 +306,26 @@ int wap_scan_debug_stall(wap_scan* scan, int pass, long long spin_limit);
  * nullable) receives [where, class, pass, probe, tile, valid] of the first
  * violation (where = 0: none). */
 int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
+/* Scheduler overrides for A/B timing and tests (no counterpart in the
+ * reference), process-wide, read by every later wap_scan_create /
+ * wap_scan_grad_create; value -1 restores the library's own choice.  Nothing
+ * else (no environment variable) changes these choices.
+ *   WAP_KNOB_ELEMS     elements per thread of forward scans: 16 or 8
+ *   WAP_KNOB_TWIDDLES  stage-twiddle table: WAP_TW_FULL (hi + lo) or WAP_TW_HI
+ *                      (hi only; by default scans of at most 160 slices)
+ *   WAP_KNOB_TW_SMEM   1: twiddles in shared memory, 0: read through L1
+ *   WAP_KNOB_PSI       how adjoint rows read psi_s: 0 global, 1 second stage,
+ *                      2 the one stage refilled (default)
+ *   WAP_KNOB_GROUP     probe-group size of classes that ask for automatic */
+#define WAP_KNOB_ELEMS 0
+#define WAP_KNOB_TWIDDLES 1
+#define WAP_KNOB_TW_SMEM 2
+#define WAP_KNOB_PSI 3
+#define WAP_KNOB_GROUP 4
+#define WAP_KNOB_COUNT 5
+#define WAP_TW_FULL 1
+#define WAP_TW_HI 2
+int wap_scan_debug_override(int which, int value);
 
 /* Kernel-level tracing (no counterpart in the reference, which has none).
  * While enabled, each pass launch is bracketed by CUDA events on its stream

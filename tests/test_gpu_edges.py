@@ -141,3 +141,41 @@ def test_transfer_split_cache_follows_changes(wap):
     e4, _, _ = wap.simulate_fresnel_as(V, psi, H.clone(), 2.0, 300e3, return_wavefronts=False)
     assert torch.equal(e3, e4)
     assert not torch.equal(e1, e3)
+
+
+def test_inference_mode_complex128_transfer(wap):
+    """Calls under torch.inference_mode() with a complex128 device transfer
+    function (an inference tensor, which has no version counter) work and give
+    the same result as outside it, on the per-pass path, the scheduler path and
+    the WPM line-transfer helper."""
+    V, probe, ps, dz, E = _setup(128, 3, seed=2)
+    pos = np.array([[64, 64], [10, 20], [100, 5], [3, 3], [64, 0], [0, 64], [127, 127], [50, 90]], np.int32)
+    H0 = wap.angular_spectrum_propagation_kernel(128, 128, (ps, ps), dz, E)
+    ref1 = wap.simulate_fresnel_as(V, probe, H0, dz, E, return_wavefronts=False)[0]
+    ref8 = wap.simulate_fresnel_as(V, probe, H0, dz, E, positions=pos, return_wavefronts=False)[0]
+    with torch.inference_mode():
+        H = wap.angular_spectrum_propagation_kernel(128, 128, (ps, ps), dz, E)
+        assert H.dtype == torch.complex128 and H.is_inference()
+        for _ in range(2):   # a second call would hit a cache entry if one had been made
+            ex1 = wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)[0]
+            ex8 = wap.simulate_fresnel_as(V, probe, H, dz, E, positions=pos, return_wavefronts=False)[0]
+            assert torch.equal(ex1, ref1) and torch.equal(ex8, ref8)
+        kp2 = torch.rand(128, 128, dtype=torch.float64, device="cuda")
+        X = torch.randn(128, 128, dtype=torch.complex64, device="cuda")
+        out = wap.wpm_propagation_kernel_vmap(X, [1.0, 1.0001], 50.0, kp2, 2.0)
+    assert torch.equal(out, wap.wpm_propagation_kernel_vmap(X, [1.0, 1.0001], 50.0, kp2, 2.0))
+
+
+def test_transfer_split_cache_other_stream(wap):
+    """A cached complex128 transfer-function split made on one stream is used
+    correctly from another stream (the consumer waits for the split)."""
+    V, probe, ps, dz, E = _setup(128, 3, seed=4)
+    H = wap.angular_spectrum_propagation_kernel(128, 128, (ps, ps), dz, E)
+    ref = wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)[0]
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        ex = wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)[0]
+    torch.cuda.current_stream().wait_stream(s)
+    assert torch.equal(ex, ref)

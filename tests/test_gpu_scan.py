@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
+from wideanglepropagation_b200 import _lib  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
@@ -119,27 +120,106 @@ def test_scan_rejects_unsupported(wap):
 
 
 @pytest.mark.parametrize("n_slices,table", [(160, "hi"), (161, "full")])
-def test_twiddle_table_gate(wap, monkeypatch, n_slices, table):
+def test_twiddle_table_gate(wap, n_slices, table):
     """Scans of at most 160 slices run the hi-only stage-twiddle table, longer
     ones hi + lo: the default run reproduces the forced table bit for bit on
     each side of the gate, and both tables stay within 1e-5 of the FP64 oracle."""
     from oracle import propagation_oracle as O
+    L = _lib.lib()
     spec = [(128, n_slices, 3, 1)]
     host = wap.synthetic.batched_scan_class(5, *spec[0])
     H = O.angular_spectrum_propagation_kernel(host.ny, host.nx, (host.ps, host.ps), host.dz, host.energy)
     p0 = O.move_probe(host.probe, tuple(host.positions[0]))
     rex, _, _ = O.simulate_fresnel_as(host.potential[0], p0, H, host.dz, host.energy, return_wavefronts=False)
-    monkeypatch.delenv("WAP_SCHED_TW", raising=False)
     ex_default, _, _ = _run(wap, _classes(wap, spec, seed=5), "persistent")
     out = {}
-    for forced in ("hi", "full"):
-        monkeypatch.setenv("WAP_SCHED_TW", forced)
-        out[forced], _, _ = _run(wap, _classes(wap, spec, seed=5), "persistent")
-        assert O.rel_l2(out[forced][0][0].cpu().numpy(), rex) < 1e-5
-    monkeypatch.delenv("WAP_SCHED_TW")
+    try:
+        for forced, knob in (("hi", _lib.WAP_TW_HI), ("full", _lib.WAP_TW_FULL)):
+            _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_TWIDDLES, knob))
+            out[forced], _, _ = _run(wap, _classes(wap, spec, seed=5), "persistent")
+            assert O.rel_l2(out[forced][0][0].cpu().numpy(), rex) < 1e-5
+    finally:
+        _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_TWIDDLES, -1))
     assert torch.equal(ex_default[0], out[table][0])
     other = "full" if table == "hi" else "hi"
     assert not torch.equal(ex_default[0], out[other][0])
+
+
+def test_scheduler_ignores_environment(wap, monkeypatch):
+    """The scheduler's choices come from the library and explicit overrides
+    only: variables in the environment change nothing."""
+    spec = [(128, 4, 8, 1)]
+    ex_default, _, _ = _run(wap, _classes(wap, spec, seed=7), "persistent")
+    for k, v in (("WAP_SCHED_TW", "full"), ("WAP_SCHED_E", "8"), ("WAP_SCHED_GROUP", "3"),
+                 ("WAP_SCHED_TWIDDLES", "global")):
+        monkeypatch.setenv(k, v)
+    ex_env, _, _ = _run(wap, _classes(wap, spec, seed=7), "persistent")
+    assert torch.equal(ex_default[0], ex_env[0])
+
+
+def test_api_raises_on_scheduler_timeout(wap):
+    """simulate_fresnel_as on the persistent scheduler raises WapError when a
+    bounded wait expires (a dependency nothing satisfies, short spin limit),
+    defers it with check=False until check_errors(), and the next call
+    succeeds with the FP64 oracle's result."""
+    from oracle import propagation_oracle as O
+    from wideanglepropagation_b200 import propagation as P
+    host = wap.synthetic.batched_scan_class(3, 128, 4, 8, 1)
+    H = wap.angular_spectrum_propagation_kernel(128, 128, (host.ps, host.ps), host.dz, host.energy)
+    args = (host.potential[0], host.probe, H, host.dz, host.energy)
+    kw = dict(positions=host.positions, return_wavefronts=False)
+    ex0, _, _ = wap.simulate_fresnel_as(*args, **kw)
+    torch.cuda.synchronize()
+    key = (torch.cuda.current_device(), 128, host.n_slices, 1, host.n_probes)
+    h = P._scans[key]
+    L = _lib.lib()
+    try:
+        _lib.check(L.wap_scan_debug_stall(h, 1, 1 << 12))
+        with pytest.raises(_lib.WapError, match="bounded device-side wait expired"):
+            wap.simulate_fresnel_as(*args, **kw)
+        wap.simulate_fresnel_as(*args, check=False, **kw)   # returns without waiting
+        with pytest.raises(_lib.WapError, match="bounded device-side wait expired"):
+            wap.check_errors()
+        wap.check_errors()   # consumed
+    finally:
+        _lib.check(L.wap_scan_debug_stall(h, -1, 0))
+    ex1, _, _ = wap.simulate_fresnel_as(*args, **kw)
+    assert torch.equal(ex0, ex1)
+    p0 = O.move_probe(host.probe, tuple(host.positions[5]))
+    rex, _, _ = O.simulate_fresnel_as(host.potential[0], p0, H.cpu().numpy(), host.dz, host.energy,
+                                      return_wavefronts=False)
+    assert O.rel_l2(ex1[5].cpu().numpy(), rex) < 1e-5
+
+
+def test_autograd_raises_on_scheduler_timeout(wap):
+    """The differentiable path on the persistent scheduler raises WapError in
+    the forward when a bounded wait expires, and works again afterwards."""
+    from wideanglepropagation_b200 import autograd as A
+    host = wap.synthetic.batched_scan_class(4, 128, 4, 8, 1)
+    H = wap.angular_spectrum_propagation_kernel(128, 128, (host.ps, host.ps), host.dz, host.energy)
+    V = torch.tensor(host.potential[0], device="cuda", requires_grad=True)
+
+    def step():
+        ex, dp = A.simulate_fresnel_as_differentiable(V, host.probe, H, host.dz, host.energy,
+                                                      positions=host.positions, ckpt_every=2)
+        dp.sum().backward()
+        g = V.grad.clone()
+        V.grad = None
+        return g
+
+    g0 = step()
+    torch.cuda.synchronize()
+    key = (torch.cuda.current_device(), 128, host.n_slices, 1, host.n_probes, 2)
+    h = A._pool[key][-1]
+    L = _lib.lib()
+    try:
+        _lib.check(L.wap_scan_debug_stall(h, 1, 1 << 12))
+        with pytest.raises(_lib.WapError, match="bounded device-side wait expired"):
+            step()
+    finally:
+        _lib.check(L.wap_scan_debug_stall(h, -1, 0))
+    g1 = step()
+    assert torch.allclose(g0, g1, rtol=1e-5, atol=1e-6 * float(g0.abs().max()))
 
 
 def test_automatic_groups_are_balanced(wap):

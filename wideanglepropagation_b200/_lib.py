@@ -24,6 +24,10 @@ WAP_OP_WPM = 1
 WAP_TF_FRESNEL = 0
 WAP_TF_ANGULAR = 1
 
+WAP_KNOB_ELEMS, WAP_KNOB_TWIDDLES, WAP_KNOB_TW_SMEM, WAP_KNOB_PSI, WAP_KNOB_GROUP = range(5)
+WAP_TW_FULL = 1
+WAP_TW_HI = 2
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
@@ -37,6 +41,8 @@ SIGNATURES = {
     "wap_plan_set_config": (_I, [_P, _I, _I, _I]),
     "wap_plan_set_detector": (_I, [_P, _I, _I, _I, _I]),
     "wap_gaussian_potential": (_I, [_I, _I, _I, _D, _D, _P, _P, _D, _D, _P, _P]),
+    "wap_aperture_probe": (_I, [_P, _D, _D, _D, _D, _D, _I, _P, _P]),
+    "wap_pattern_accumulate": (_I, [_P, _I, ctypes.c_longlong, _P, _P, _I, _P, _P, _P]),
     "wap_spectrum_propagate": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "wap_scan_grad_backward_ex": (_I, [_P, _P, _P, _P, _P]),
     "wap_fp32_probe": (_I, [_I, _I, _P, _P]),
@@ -57,6 +63,8 @@ SIGNATURES = {
     "wap_scan_grad_backward": (_I, [_P, _P, _P, _P]),
     "wap_scan_bind": (_I, [_P, _I, _P]),
     "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
+    "wap_scan_status_async": (_I, [_P, _P, _P]),
+    "wap_scan_debug_override": (_I, [_I, _I]),
     "wap_scan_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_scan_destroy": (_I, [_P]),
     "wap_scan_debug_stall": (_I, [_P, _I, ctypes.c_longlong]),
@@ -117,6 +125,72 @@ def check(rc: int) -> None:
     if rc in (WAP_ERR_ARG, WAP_ERR_UNSUPPORTED):
         raise ValueError(msg)
     raise WapError(f"libwap error {rc}: {msg}")
+
+
+# Device-side status of persistent-scheduler runs whose check was deferred
+# (check=False): (event after the status copy, pinned host word, what ran).
+_pending: list = []
+_pending_lock = threading.Lock()
+
+
+def scan_status_begin(handle, what: str):
+    """Enqueue, on the current stream, a copy of a scan's status word into
+    pinned host memory and record an event after it; returns the token that
+    ``scan_status_end`` or ``defer_status`` take."""
+    import torch
+    word = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+    stream = torch.cuda.current_stream()
+    check(lib().wap_scan_status_async(handle, ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
+    ev = torch.cuda.Event()
+    ev.record(stream)
+    return ev, word, what
+
+
+def _raise_status(token) -> None:
+    ev, word, what = token
+    ev.synchronize()
+    st = int(word[0])
+    if st != WAP_OK:
+        kind = "a bounded device-side wait expired" if st == WAP_ERR_TIMEOUT else "the kernel reported an error"
+        raise WapError(f"libwap error {st}: {what}: {kind}; its outputs are incomplete")
+
+
+def scan_status_end(token) -> None:
+    """Wait for the status copy of ``token`` and raise WapError if the run failed."""
+    _raise_status(token)
+
+
+def defer_status(token) -> None:
+    """Keep ``token`` for ``check_errors`` (and the next checked call)."""
+    with _pending_lock:
+        _pending.append(token)
+
+
+def check_errors() -> None:
+    """Wait for every deferred scheduler status and raise WapError for the
+    first run that failed (all deferred statuses are consumed)."""
+    with _pending_lock:
+        tokens = list(_pending)
+        _pending.clear()
+    first = None
+    for t in tokens:
+        try:
+            _raise_status(t)
+        except WapError as e:
+            first = first or e
+    if first is not None:
+        raise first
+
+
+def poll_errors() -> None:
+    """Raise WapError for a deferred run that has already finished and failed;
+    never blocks (runs still in flight stay pending)."""
+    with _pending_lock:
+        done = [t for t in _pending if t[0].query()]
+        for t in done:
+            _pending.remove(t)
+    for t in done:
+        _raise_status(t)
 
 
 def version() -> str:

@@ -89,7 +89,7 @@ class _Lease:
 
 class MultisliceFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every, det):
+    def forward(ctx, V, probe, H, dz, energy, positions, draw, ckpt_every, det, check=True):
         dev = V.device
         ctx.set_materialize_grads(False)
         Vc, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(V.detach(), probe, positions, draw, dev)
@@ -104,6 +104,12 @@ class MultisliceFunction(torch.autograd.Function):
             h = _acquire(key, scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp, det), k)
             _lib.check(_lib.lib().wap_scan_run(h, _stream()))
             ctx.scan = _Lease(key, h)
+            ctx.check = check
+            token = _lib.scan_status_begin(h, f"gradient scan forward of {B} probes on {ny}x{nx}, {N} slices")
+            if check:
+                _lib.scan_status_end(token)
+            else:
+                _lib.defer_status(token)
             # everything the scan reads in the backward must outlive it.  The
             # exit wave is an output: it goes through save_for_backward (a
             # plain attribute would tie output -> graph -> ctx -> output in a
@@ -142,12 +148,18 @@ class MultisliceFunction(torch.autograd.Function):
             try:
                 grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=Vc.device)
                 if g_exit is None and g_dp is None:
-                    return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
+                    return grad_V.reshape(vshape), None, None, None, None, None, None, None, None, None
                 g = None if g_dp is None else g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
                 ge = None if g_exit is None else g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
                 _lib.check(_lib.lib().wap_scan_grad_backward_ex(lease.h, _ptr(g), _ptr(ge), _ptr(grad_V),
                                                                 _stream()))
-                return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
+                token = _lib.scan_status_begin(lease.h, f"gradient scan backward of {B} probes on {ny}x{nx}, "
+                                                        f"{N} slices")
+                if ctx.check:
+                    _lib.scan_status_end(token)
+                else:
+                    _lib.defer_status(token)
+                return grad_V.reshape(vshape), None, None, None, None, None, None, None, None, None
             finally:
                 lease.release()
         Vc, Hc, Hl, exit_wave, ckpt, dr = ctx.saved_tensors
@@ -165,19 +177,23 @@ class MultisliceFunction(torch.autograd.Function):
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr) if has_draw else None, B, _ptr(Hc),
             _ptr(Hl) if Hl.numel() else None, dz, energy,
             _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
-        return grad_V.reshape(vshape), None, None, None, None, None, None, None, None
+        return grad_V.reshape(vshape), None, None, None, None, None, None, None, None, None
 
 
 def simulate_fresnel_as_differentiable(potential: torch.Tensor, probe, prop_kernel, slice_thickness, energy, *,
                                        positions=None, draw=None, ckpt_every: int | None = None,
-                                       max_angle=None, sampling=None, parity="odd"):
+                                       max_angle=None, sampling=None, parity="odd", check: bool = True):
     """(exit_wave, diffraction_pattern) with gradients flowing to ``potential``.
 
     ``ckpt_every`` defaults to round(sqrt(N)) slices between saved waves.
     ``max_angle`` / ``sampling`` / ``parity``: the pattern is cropped to the
     detector window as in ``simulate_fresnel_as`` (the loss sees only it).
+    On the persistent scheduler the forward and the backward raise WapError
+    if a bounded device-side wait expired; ``check=False`` defers that to
+    ``check_errors()`` (or the next call) instead of waiting for the GPU.
     """
     _device()
+    _lib.poll_errors()
     if not isinstance(potential, torch.Tensor):
         raise TypeError("potential must be a torch tensor to differentiate")
     N = potential.shape[-3]
@@ -185,4 +201,4 @@ def simulate_fresnel_as_differentiable(potential: torch.Tensor, probe, prop_kern
         ckpt_every = max(1, int(round(math.sqrt(N))))
     det = _detector(tuple(potential.shape[-2:]), sampling, energy, max_angle, parity)
     return MultisliceFunction.apply(potential, probe, prop_kernel, slice_thickness, energy, positions, draw,
-                                    ckpt_every, det)
+                                    ckpt_every, det, check)

@@ -1058,6 +1058,12 @@ static void scan_free(wap_scan* s) {
 
 static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n == 1024; }
 
+// Scheduler overrides for A/B timing and tests (wap_scan_debug_override); -1:
+// the library's own choice.  Set only by an explicit call, never from the
+// environment, and read when a scan is created.
+static int g_knob[WAP_KNOB_COUNT] = {-1, -1, -1, -1, -1};
+static int knob(int k) { return g_knob[k]; }
+
 static bool windowed(const Detector& d, int n) { return d.ny != n || d.nx != n; }
 
 // detector window of a class's diffraction patterns (0 x 0: the whole grid)
@@ -1247,9 +1253,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
   // elements per thread of the scheduler's transforms (16; 8 for A/B timing)
   int E = 16;
-  if (const char* ov = getenv("WAP_SCHED_E")) {
-    if (!strcmp(ov, "8") && !s->grad) E = 8;
-  }
+  if (knob(WAP_KNOB_ELEMS) == 8 && !s->grad) E = 8;
   s->e = E;
   // Hi-only stage twiddles: each entry's float rounding repeats in every
   // transform, so its error grows linearly with the slices a wave crosses
@@ -1261,10 +1265,8 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   int max_slices = 0;
   for (int ci = 0; ci < n_classes; ++ci) max_slices = std::max(max_slices, classes[ci].n_slices);
   s->hi_tw = E == 16 && max_slices <= kHiTwiddleMaxSlices;
-  if (const char* ov = getenv("WAP_SCHED_TW")) {   // A/B timing and error checks only
-    if (!strcmp(ov, "full")) s->hi_tw = false;
-    if (!strcmp(ov, "hi")) s->hi_tw = E == 16;
-  }
+  if (knob(WAP_KNOB_TWIDDLES) == WAP_TW_FULL) s->hi_tw = false;
+  if (knob(WAP_KNOB_TWIDDLES) == WAP_TW_HI) s->hi_tw = E == 16;
   unsigned mask = 0;
   for (int ci = 0; ci < n_classes; ++ci) {
     const int n = classes[ci].n;
@@ -1320,20 +1322,15 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   if ((rc0 = ctas_per_sm(s->kernel, base_smem, &per_sm)) || (rc0 = ctas_per_sm(s->kernel, base_smem + tw_smem_bytes, &per_sm_tw)))
     return rc0;
   s->params.tw_in_smem = per_sm_tw >= per_sm && per_sm_tw > 0;
-  if (const char* ov = getenv("WAP_SCHED_TWIDDLES")) {   // debugging / A-B timing only
-    if (!strcmp(ov, "smem")) s->params.tw_in_smem = 1;
-    if (!strcmp(ov, "global")) s->params.tw_in_smem = 0;
-  }
+  if (knob(WAP_KNOB_TW_SMEM) >= 0) s->params.tw_in_smem = knob(WAP_KNOB_TW_SMEM) != 0;
   s->smem = base_smem + (s->params.tw_in_smem ? tw_smem_bytes : 0);
   if ((rc0 = ctas_per_sm(s->kernel, s->smem, &per_sm))) return rc0;
   if (per_sm < 1) return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
   s->grid = sms * per_sm;
   if (s->grad) {
     // kPsiStage2 stages psi_s next to lambda: one more tile of shared memory
-    if (const char* ov = getenv("WAP_SCHED_PSI")) {   // A/B timing only
-      const int m = atoi(ov);
-      if (m >= kPsiGlobal && m <= kPsiSplit) s->psi_mode = m;
-    }
+    const int m = knob(WAP_KNOB_PSI);
+    if (m >= kPsiGlobal && m <= kPsiSplit) s->psi_mode = m;
     s->smem_bwd = s->smem + (s->psi_mode == kPsiStage2 ? kTileBytesFor(E) : 0);
     int per_sm_bwd = 0;
     if ((rc0 = ctas_per_sm(s->kernel_bwd, s->smem_bwd, &per_sm_bwd))) return rc0;
@@ -1440,9 +1437,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     forward_steps(sc, c.n_slices, ckpt_every, steps);
     if (s->grad) backward_steps(sc, c.n_slices, ckpt_every, steps_bwd);
     int G = c.group;
-    if (const char* ov = getenv("WAP_SCHED_GROUP")) {   // A/B timing only
-      if (G <= 0) G = atoi(ov);
-    }
+    if (G <= 0 && knob(WAP_KNOB_GROUP) > 0) G = knob(WAP_KNOB_GROUP);
     if (G <= 0) {
       // enough tiles per step to cover the resident CTAs four times (a
       // group's steps are a dependency chain, so this is the parallelism
@@ -1732,6 +1727,21 @@ int wap_scan_status(wap_scan* s, int* status) {
   if (e != cudaSuccess) return cuda_fail(e, "scan status");
   *status = h;
   if (h != 0) return fail(h, "scan kernel reported status %d (a bounded wait expired)", h);
+  return WAP_OK;
+}
+
+int wap_scan_status_async(wap_scan* s, int* host_status, void* stream) {
+  clear_error();
+  if (!s || !host_status) return fail(WAP_ERR_ARG, "NULL argument");
+  cudaError_t e = cudaMemcpyAsync(host_status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "scan status copy");
+  return WAP_OK;
+}
+
+int wap_scan_debug_override(int which, int value) {
+  clear_error();
+  if (which < 0 || which >= WAP_KNOB_COUNT) return fail(WAP_ERR_ARG, "unknown scheduler override %d", which);
+  g_knob[which] = value < 0 ? -1 : value;
   return WAP_OK;
 }
 

@@ -47,6 +47,7 @@ __all__ = [
     "simulate_fresnel_as_jit", "simulate_fresnel", "simulate_wpm",
     "simulate_wpm_jit", "max_angle_gpts", "downsample_to_max_angle", "detector_window",
     "wpm_propagation_kernel", "wpm_propagation_kernel_vmap", "get_abtem_transmit", "release_caches",
+    "check_errors", "accumulate_patterns", "aperture_probe",
 ]
 
 
@@ -94,39 +95,59 @@ def _to(x, dtype, device) -> torch.Tensor:
 
 
 # Recent splits of complex128 device tensors: (source tensor, its version,
-# device, hi, lo).  An entry keeps its source alive, so no other tensor can
-# take its memory while cached, and an in-place change of the source bumps
-# its version and misses.
+# device, hi, lo, event recorded after the split on the stream that made it).
+# An entry keeps its source alive, so no other tensor can take its memory
+# while cached, and an in-place change of the source bumps its version and
+# misses.  Inference tensors carry no version counter and are never cached.
 _SPLIT_CACHE_MAX = 4
 _split_cache: list = []
 _split_lock = threading.Lock()
 
 
-def split_transfer(H, device):
+def _version_of(t: torch.Tensor):
+    """The tensor's version counter, or None where it has none (inference tensors)."""
+    if t.is_inference():
+        return None
+    try:
+        return t._version
+    except RuntimeError:
+        return None
+
+
+def split_transfer(H, device, cache: bool = True):
     """complex64 hi part and remainder of a transfer function.
 
     A complex128 H is split into H_hi = (complex64)H and H_lo = H - H_hi; the
     kernels apply X*H_hi + X*H_lo, which removes the rounding of H that would
     otherwise repeat identically at every slice.  A complex64 H has no lo part.
     A complex128 tensor already on the device is split once and reused while
-    it is unchanged (a transfer function normally serves many calls).
+    it is unchanged (a transfer function normally serves many calls); a caller
+    on another stream than the one that made the split waits for it first.
+    ``cache=False`` (internal scratch that the kernels rewrite) always splits.
     """
     t = H if isinstance(H, torch.Tensor) else torch.as_tensor(np.asarray(H))
     if t.dtype == torch.complex128:
         dev = torch.device(device)
-        cacheable = t.device.type == "cuda" and t.device == dev
+        ver = _version_of(t) if cache else None
+        cacheable = ver is not None and t.device.type == "cuda" and t.device == dev
         if cacheable:
             with _split_lock:
-                for i, (src, ver, d, hi, lo) in enumerate(_split_cache):
-                    if src is t and ver == t._version and d == dev:
+                for i, (src, sver, d, hi, lo, ev) in enumerate(_split_cache):
+                    if src is t and sver == ver and d == dev:
                         _split_cache.append(_split_cache.pop(i))
+                        cur = torch.cuda.current_stream(dev)
+                        cur.wait_event(ev)
+                        hi.record_stream(cur)
+                        lo.record_stream(cur)
                         return hi, lo
         t = t.to(device)
         hi = t.to(torch.complex64).contiguous()
         lo = (t - hi.to(torch.complex128)).to(torch.complex64).contiguous()
         if cacheable:
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(dev))
             with _split_lock:
-                _split_cache.append((H, H._version, dev, hi, lo))
+                _split_cache.append((H, ver, dev, hi, lo, ev))
                 del _split_cache[:-_SPLIT_CACHE_MAX]
         return hi, lo
     return _to(t, torch.complex64, device), None
@@ -347,10 +368,17 @@ def _prepare(potential, probe, positions, draw, dev):
         raise ValueError("positions and batched probe disagree on the batch size")
     dr = None
     if draw is not None:
+        # host arrays are range-checked before the upload (no device sync);
+        # a device tensor is checked on the device
+        on_host = not isinstance(draw, torch.Tensor) or draw.device.type == "cpu"
+        if on_host:
+            d = draw.reshape(-1) if isinstance(draw, torch.Tensor) else np.asarray(draw).reshape(-1)
+            if d.shape[0] == B and d.shape[0] > 0 and (int(d.min()) < 0 or int(d.max()) >= n_draws):
+                raise ValueError("draw index out of range")
         dr = _to(draw, torch.int32, dev).reshape(-1)
         if dr.shape[0] != B:
             raise ValueError("draw must have one entry per probe")
-        if int(dr.min()) < 0 or int(dr.max()) >= n_draws:
+        if not on_host and (int(dr.min()) < 0 or int(dr.max()) >= n_draws):
             raise ValueError("draw index out of range")
     elif n_draws > 1:
         raise ValueError("a potential with several draws needs `draw`")
@@ -386,6 +414,44 @@ def _dp_shape(B, ny, nx, det):
     return (B, det[2], det[3]) if det is not None else (B, ny, nx)
 
 
+def _accumulation(accumulate, B, dev):
+    """Host-validated CSR of ``accumulate`` ((B,) pattern index per probe):
+    (n_patterns, start (P+1,) int32, probes (B,) int32) on the device, the
+    probes of each pattern in increasing order."""
+    idx = accumulate.cpu().numpy() if isinstance(accumulate, torch.Tensor) else np.asarray(accumulate)
+    idx = idx.reshape(-1)
+    if idx.shape[0] != B:
+        raise ValueError(f"accumulate needs one pattern index per probe ({B}), got {idx.shape[0]}")
+    if not np.issubdtype(idx.dtype, np.integer):
+        raise ValueError("accumulate must hold integer pattern indices")
+    if idx.size and idx.min() < 0:
+        raise ValueError("accumulate indices must be >= 0")
+    P = int(idx.max()) + 1 if idx.size else 0
+    order = np.argsort(idx, kind="stable").astype(np.int32)
+    start = np.concatenate([[0], np.cumsum(np.bincount(idx, minlength=P))]).astype(np.int32)
+    return P, torch.as_tensor(start).to(dev), torch.as_tensor(order).to(dev)
+
+
+def accumulate_patterns(dp: torch.Tensor, accumulate) -> torch.Tensor:
+    """Sum per-probe diffraction patterns ``dp`` (B, ...) into
+    (max(accumulate) + 1, ...) patterns: pattern p is the float32 sum of the
+    patterns of the probes b with ``accumulate[b] == p``, added in increasing b
+    (deterministic).  The incoherent frozen-phonon average per scan position
+    that the reference's callers form by summing simulate_fresnel_as patterns
+    over configurations, as one device kernel (``wap_pattern_accumulate``)."""
+    dev = dp.device
+    B = dp.shape[0]
+    P, start, order = _accumulation(accumulate, B, dev)
+    plane = int(np.prod(dp.shape[1:]))
+    dpc = dp.contiguous()
+    out = torch.empty((P,) + tuple(dp.shape[1:]), dtype=torch.float32, device=dev)
+    if P == 0:
+        return out
+    _lib.check(_lib.lib().wap_pattern_accumulate(_ptr(dpc), B, plane, _ptr(start), _ptr(order), P, _ptr(out), None,
+                                                 _stream()))
+    return out
+
+
 def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, group=None):
     """``wap_scan_class`` for one grid class of device tensors; the probe-group
     size defaults to the autotuned one for the grid (0: the scheduler's own)."""
@@ -401,8 +467,14 @@ def scan_class(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, gr
                           y0, x0, dny, dnx)
 
 
-def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None):
-    """Run a batched forward through the persistent scheduler (cached per shape)."""
+def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, check=True):
+    """Run a batched forward through the persistent scheduler (cached per shape).
+
+    The scheduler's bounded waits report an expiry in a device status word
+    instead of faulting.  ``check=True`` waits for the run and raises WapError
+    if a wait expired; ``check=False`` returns at once and leaves the status
+    to ``check_errors()`` (or to the next call, which raises for any finished
+    deferred run that failed)."""
     D, N, n, _ = V.shape
     B = exit_wave.shape[0]
     dev = torch.cuda.current_device()
@@ -420,6 +492,17 @@ def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None):
         else:
             _lib.check(L.wap_scan_bind(h, 1, arr))
         _lib.check(L.wap_scan_run(h, _stream()))
+        token = _lib.scan_status_begin(h, f"persistent scan of {B} probes on {n}x{n}, {N} slices")
+    if check:
+        _lib.scan_status_end(token)
+    else:
+        _lib.defer_status(token)
+
+
+def check_errors() -> None:
+    """Raise WapError for a scheduler run issued with ``check=False`` whose
+    bounded waits expired (waits for those runs; clears them)."""
+    _lib.check_errors()
 
 
 def release_caches() -> None:
@@ -444,7 +527,7 @@ def release_caches() -> None:
 
 def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, *,
                         return_wavefronts: bool = True, positions=None, draw=None,
-                        max_angle=None, sampling=None, parity="odd"):
+                        max_angle=None, sampling=None, parity="odd", check: bool = True, accumulate=None):
     """Fresnel / angular-spectrum multislice (propagation.py:305-352).
 
     Returns ``(exit_wave, diffraction_pattern, wavefronts)`` where
@@ -453,8 +536,18 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     ``return_wavefronts=False``).  With ``max_angle`` (mrad) and ``sampling``
     the pattern is ``downsample_to_max_angle(pattern, sampling,
     wavelength, max_angle, parity)``, stored cropped by the kernel.
+
+    ``accumulate`` ((B,) ints): the returned patterns are summed per index
+    (``accumulate_patterns``), e.g. the frozen-phonon draws of each scan
+    position into one float32 pattern per position; exit waves stay per probe.
+
+    Calls that run on the persistent scheduler (many probes of one probe)
+    raise WapError if one of its bounded device-side waits expired; with
+    ``check=False`` the call returns without waiting for the GPU and the
+    failure is raised by ``check_errors()`` or by a later call.
     """
     dev = _device()
+    _lib.poll_errors()
     V, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(potential, probe, positions, draw, dev)
     if N < 1:
         raise ValueError("need at least one array to stack")  # jnp.stack([]) in the reference
@@ -467,7 +560,9 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     if (not return_wavefronts and ny == nx and ny in SCAN_SIZES and B >= SCAN_MIN_PROBES
             and not per_probe):
         # many probes of one shared probe: the persistent batched scheduler
-        _scan_run(V, psi, pos, dr, H, H_lo, slice_thickness, energy, exit_wave, dp, det)
+        _scan_run(V, psi, pos, dr, H, H_lo, slice_thickness, energy, exit_wave, dp, det, check=check)
+        if accumulate is not None:
+            dp = accumulate_patterns(dp, accumulate)
         if not batched:
             exit_wave, dp = exit_wave[0], dp[0]
         return exit_wave, dp, None
@@ -478,6 +573,8 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), _ptr(H), _ptr(H_lo), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
         _ptr(stack), _stream()))
+    if accumulate is not None:
+        dp = accumulate_patterns(dp, accumulate)
     if not batched:
         exit_wave, dp = exit_wave[0], dp[0]
         stack = stack[0] if stack is not None else None
@@ -490,7 +587,8 @@ simulate_fresnel = simulate_fresnel_as
 
 
 def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128, power_spacing=2.0, *,
-                 return_wavefronts: bool = True, positions=None, draw=None, max_angle=None, parity="odd"):
+                 return_wavefronts: bool = True, positions=None, draw=None, max_angle=None, parity="odd",
+                 accumulate=None):
     """WPM adaptive-binning multislice (propagation.py:358-387).
 
     Per slice: n_bins reference refractive indices spaced
@@ -498,6 +596,7 @@ def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128
     per reference, smoothstep blend of the two bracketing fields per pixel
     (propagation.py:215-256).  ``sampling`` = (dy, dx).  ``max_angle`` (mrad):
     the pattern comes back cropped as by ``downsample_to_max_angle``.
+    ``accumulate``: patterns summed per index, as in ``simulate_fresnel_as``.
     """
     dev = _device()
     V, psi, per_probe, pos, dr, B, N, ny, nx, batched = _prepare(potential, probe, positions, draw, dev)
@@ -517,6 +616,8 @@ def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), float(slice_thickness), float(energy), dy, dx, float(power_spacing),
         _ptr(exit_wave), _ptr(dp), _ptr(stack), _stream()))
+    if accumulate is not None:
+        dp = accumulate_patterns(dp, accumulate)
     if not batched:
         exit_wave, dp = exit_wave[0], dp[0]
         stack = stack[0] if stack is not None else None
@@ -558,7 +659,7 @@ def wpm_propagation_kernel_vmap(Ek, n_vals, k0, k_perp2, dz) -> torch.Tensor:
     for i, n in enumerate(nv):
         _lib.check(L.wap_line_transfer(_lib.WAP_TF_ANGULAR, ny * nx, _ptr(kp2), float(n) * float(k0), float(dz),
                                        _ptr(H), _stream()))
-        Hh, Hl = split_transfer(H.view(ny, nx), dev)
+        Hh, Hl = split_transfer(H.view(ny, nx), dev, cache=False)
         _lib.check(L.wap_spectrum_propagate(plan.handle, _ptr(X), 1, _ptr(Hh), _ptr(Hl), _ptr(out[i]), _stream()))
     return out
 
@@ -566,6 +667,26 @@ def wpm_propagation_kernel_vmap(Ek, n_vals, k0, k_perp2, dz) -> torch.Tensor:
 def wpm_propagation_kernel(Ek, n_val, k0, k_perp2, dz) -> torch.Tensor:
     """One homogeneous-index WPM propagate of a spectrum (propagation.py:159-167)."""
     return wpm_propagation_kernel_vmap(Ek, [float(n_val)], k0, k_perp2, dz)[0]
+
+
+def aperture_probe(ny: int, nx: int, sampling, energy: float, alpha_mrad: float, defocus: float = 0.0,
+                   centred: bool = True) -> torch.Tensor:
+    """Convergent probe built on the device: (ny, nx) complex64.
+
+    A hard aperture |f| lambda < alpha with the defocus phase
+    exp(-i pi lambda df |f|^2) inside it (float64), inverse-transformed by the
+    library's transforms, normalised to sum |psi|^2 = ny nx and, if
+    ``centred``, rolled to the grid centre (the origin ``move_probe``
+    measures positions from).  The reference's callers build probes on the
+    host with abTEM (e.g. wpm/cbed.ipynb); this is the probe model of the
+    benchmark configurations, without a host round trip."""
+    dev = _device()
+    ps_y, ps_x = _pair(sampling)
+    plan = get_plan(int(ny), int(nx), 1, _lib.WAP_OP_FRESNEL_AS)
+    out = torch.empty((int(ny), int(nx)), dtype=torch.complex64, device=dev)
+    _lib.check(_lib.lib().wap_aperture_probe(plan.handle, ps_y, ps_x, float(energy), float(alpha_mrad),
+                                             float(defocus), 1 if centred else 0, _ptr(out), _stream()))
+    return out
 
 
 def get_abtem_transmit(potential, energy):
