@@ -23,8 +23,11 @@ Printed JSON line (rank 0):
   cpu_baseline  the NumPy/SciPy FP64 restatement on the host cores
 
 ``--impl reference`` times that CPU restatement alone as the reference arm.
-Multi-GPU (torchrun): every rank runs its own copy of the scan (probes shard
-with no data-path collective): weak scaling, max over ranks.
+Multi-GPU (torchrun): the 1088 probes are sharded across the ranks in
+contiguous blocks per grid class (strong scaling: the whole job's work is
+fixed), no collective inside the multislice; the e2e leg runs the sharded
+public API (frozen-phonon draws summed per position on the rank that owns the
+position) and each rank downloads its own patterns; time = max over ranks.
 """
 from __future__ import annotations
 
@@ -69,6 +72,11 @@ def parse():
                          "size, roofline fraction; prints one JSON object")
     ap.add_argument("--mode", default="persistent", choices=["persistent", "batched", "graph"],
                     help="batched execution mode timed as the headline")
+    ap.add_argument("--traffic-case", action="store_true",
+                    help="DRAM-traffic case for ncu counter captures: the headline classes at their full slice "
+                         "counts with fewer probes (228 on 256^2 = two probe groups of 114, 32 on 512^2 = one "
+                         "group), one warm-up and one step, no extras; the library's bytes per pixel-slice-step "
+                         "are the same per probe group as in the full step")
     ap.add_argument("--profile-case", action="store_true",
                     help="reduced scan for ncu captures: 512 probes 256^2 x 4 slices + 32 probes 512^2 x 4 "
                          "slices (waves 256 + 64 MB, above L2), one warm-up and one step, no extras")
@@ -93,12 +101,14 @@ def cpu_reference_sample(classes_host, scale=1, mode="fp64"):
     """Time the oracle restatement on a bounded sample of each grid class
     (16*scale probes of the 256^2 class, 2*scale of the 512^2 class, 8 slices).
 
-    Returns (slice-steps/s for the workload mix, cores, sample description)."""
+    Returns (slice-steps/s for the workload mix, cores, sample description,
+    seconds the sample took, slice-steps in the sample)."""
     from oracle import propagation_oracle as O
     cores = os.cpu_count() or 1
     O.set_workers(cores)
     per_step = []
     desc = []
+    wall, steps = 0.0, 0
     for w in classes_host:
         H = O.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
         nb = (16 if w.ny <= 256 else 2) * scale
@@ -107,26 +117,39 @@ def cpu_reference_sample(classes_host, scale=1, mode="fp64"):
         t0 = time.perf_counter()
         O.simulate_fresnel_as(w.potential[0, :ns], probes, H, w.dz, w.energy, mode=mode, return_wavefronts=False)
         dt = time.perf_counter() - t0
+        wall += dt
+        steps += nb * ns
         per_step.append(dt / (nb * ns))
         desc.append(f"{nb} probes x {ns} slices at {w.ny}^2")
     rate = mix_rate(per_step, [w.n_probes * w.n_slices for w in classes_host])
-    return rate, cores, "; ".join(desc) + f" (oracle {mode}, scipy.fft workers={cores}), scaled to the workload mix"
+    return (rate, cores, "; ".join(desc) + f" (oracle {mode}, scipy.fft workers={cores}), scaled to the workload mix",
+            wall, steps)
 
 
 def run_reference(args, classes_host, rank):
+    """The reference arm: the CPU restatement on a bounded sample per step.
+    ``ms_per_step`` is the measured wall time of one sample (what each of the
+    timed steps ran); ``value`` scales the sample's per-class rates to the
+    workload mix (the full workload is not run on the host)."""
     if rank != 0:
         return
-    rates = []
+    rates, walls = [], []
     for i in range(args.warmup + args.steps):
-        r, cores, desc = cpu_reference_sample(classes_host)
+        r, cores, desc, wall, steps = cpu_reference_sample(classes_host)
         if i >= args.warmup:
             rates.append(r)
+            walls.append(wall)
     v = statistics.median(rates)
+    total = sum(c.n_probes * c.n_slices for c in classes_host)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "slice-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(c.n_probes * c.n_slices for c in classes_host) / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls),
+            "ms_per_step_note": (f"measured wall time of one step's sample ({steps} slice-steps); value scales the "
+                                 f"sample's per-class rates to the {total}-slice-step workload mix, which would take "
+                                 f"{total / v:.1f} s per step on these cores"),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic", "config": {"workload": WORKLOAD},
-            "cpu_baseline": {"value": v, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc},
+            "cpu_baseline": {"value": v, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc,
+                             "sample_s": statistics.median(walls), "sample_slice_steps": steps},
             "e2e": {"value": v, "unit": "slice-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -211,12 +234,24 @@ def main():
     if args.profile_case:
         classes_host = [S.batched_scan_class(0, 256, 4, 16, 2), S.batched_scan_class(1, 512, 4, 4, 2)]
         args.steps, args.warmup, args.no_extras = 1, 1, True
+    elif args.traffic_case:
+        import dataclasses
+        full = S.batched_scan(0)
+        classes_host = [dataclasses.replace(full[0], positions=full[0].positions[:228],
+                                            draw_of_probe=full[0].draw_of_probe[:228]),
+                        dataclasses.replace(full[1], positions=full[1].positions[:32],
+                                            draw_of_probe=full[1].draw_of_probe[:32])]
+        args.steps, args.warmup, args.no_extras = 1, 1, True
     else:
         classes_host = S.batched_scan(0, small=args.small)
 
     if args.impl == "reference":
         run_reference(args, classes_host, rank)
         return
+    total_ss_job = sum(w.n_probes * w.n_slices for w in classes_host)
+    job_classes = classes_host
+    if world > 1:
+        classes_host = [_shard_class(w, rank, world) for w in classes_host]
 
     import torch
     import torch.distributed as dist
@@ -268,7 +303,7 @@ def main():
     barrier()
     ms = max_over_ranks(start.elapsed_time(stop))
     ms_per_step = ms / args.steps
-    value = total_ss * world / (ms_per_step / 1e3)
+    value = total_ss_job / (ms_per_step / 1e3)
     gpu_launches = (l1 - l0) + graph_launches
 
     extras = {}
@@ -290,9 +325,11 @@ def main():
     peak, peak_src = _peak_hbm()
     achieved = by / (kms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": _ncu_traffic(dom), "kernel": dom, "peak_source": peak_src,
+                "traffic": None, "kernel": dom, "peak_source": peak_src,
                 "launches": n, "avg_launch_us": 1e3 * kms / n,
                 "share": {k: v[1] / sum(x[1] for x in kinds.values()) for k, v in kinds.items()}}
+    roofline["traffic"], roofline["traffic_source"] = _ncu_traffic(
+        dom, sum(w.n_probes * w.n_slices * w.ny * w.nx for w in classes_host))
     # FP32 side: algorithmic flops of one launch (10 N log2 N + 24 N per
     # slice-step of an N-pixel Fresnel/AS grid) against the measured FMA peak;
     # time_frac = max(bytes / HBM peak, flops / FP32 peak) / launch time
@@ -324,30 +361,41 @@ def main():
         extras.update(_lippmann_schwinger())
 
     # --- e2e through the public API from pinned host buffers ------------------
-    e2e = _e2e(classes_host, args, dev, barrier, max_over_ranks, world)
+    e2e = _e2e(job_classes, args, dev, barrier, max_over_ranks, world, rank)
     if extras_on:
         # the same with a 50 mrad detector: the crop is fused into the last column pass
-        extras["e2e_detector_50mrad"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=50.0)
-        # the same from atom lists: the potential is built on the device
-        extras["e2e_from_atoms"] = _e2e(classes_host, args, dev, barrier, max_over_ranks, world, from_atoms=True)
+        extras["e2e_detector_50mrad"] = _e2e(job_classes, args, dev, barrier, max_over_ranks, world, rank,
+                                             max_angle=50.0)
+        # the same from atom lists: the potential and the probe are built on the device
+        extras["e2e_from_atoms"] = _e2e(job_classes, args, dev, barrier, max_over_ranks, world, rank,
+                                        from_atoms=True)
+        # per-probe patterns (no per-position accumulation of the draws)
+        extras["e2e_per_probe_patterns"] = _e2e(job_classes, args, dev, barrier, max_over_ranks, world, rank,
+                                                accumulate=False)
 
     cpu = None
     if rank == 0 and extras_on:
-        r, cores, desc = cpu_reference_sample(classes_host, scale=4, mode="fp64")
-        cpu = {"value": r, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc}
+        r, cores, desc, wall, steps = cpu_reference_sample(classes_host, scale=4, mode="fp64")
+        cpu = {"value": r, "unit": "slice-steps/s", "cores": cores, "kind": "port", "sample": desc,
+               "sample_s": wall, "sample_slice_steps": steps}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "slice-steps/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak",
                 "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "slice_steps_per_step": total_ss,
-                           "pixel_slice_steps_per_step": sum(c.pixel_slice_steps for c in classes),
+                "config": {"workload": WORKLOAD, "slice_steps_per_step": total_ss_job,
+                           "pixel_slice_steps_per_step": sum(w.n_probes * w.n_slices * w.ny * w.nx
+                                                             for w in job_classes),
                            "l2": "inputs larger than L2 (potential 241 MB, waves 640 MB per step)",
                            "mode": {"persistent": "one persistent kernel per step (device ticket queue, TMA tiles), "
                                                   "CUDA-graph replay",
                                     "batched": "per-pass launches over all probes of a class",
                                     "graph": "per-pass launches, CUDA-graph replay"}[args.mode],
-                           "parallelism": f"probe shards x{world}"},
+                           "parallelism": f"probe shards x{world}" + (" (strong scaling: the job's probes split "
+                                                                      "across ranks)" if world > 1 else ""),
+                           "patterns": "e2e: the 4 frozen-phonon draws of each 256^2 position summed in float32 "
+                                       "(one pattern per position); the 512^2 class has one draw"},
                 "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clk,
                 "cpu_baseline": cpu}
         line.update(extras)
@@ -356,19 +404,41 @@ def main():
         dist.destroy_process_group()
 
 
-def _ncu_traffic(kernel):
-    """DRAM bytes per launch of ``kernel`` from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+def _sources_sha256():
+    """Digest of the library's CUDA sources and C header (the build a profile
+    was taken on)."""
+    import glob
+    import hashlib
+    h = hashlib.sha256()
+    files = sorted(glob.glob(os.path.join(ROOT, "wideanglepropagation_b200", "csrc", "*"))) + \
+        [os.path.join(ROOT, "include", "wap.h")]
+    for f in files:
+        h.update(os.path.basename(f).encode())
+        h.update(open(f, "rb").read())
+    return h.hexdigest()
+
+
+def _ncu_traffic(kernel, pixel_slice_steps):
+    """DRAM bytes per launch of ``kernel``: the committed ncu record's bytes per
+    pixel-slice-step (a capture of --traffic-case) times this launch's
+    pixel-slice-steps, with where it came from; traffic None when the record
+    was taken on other library sources than these."""
+    p = os.path.join(ROOT, "profiles", "scan_kernel_dram_traffic.txt")
     if not os.path.exists(p):
-        return None
+        return None, "no committed DRAM-traffic record"
+    rec = {}
     for line in open(p):
-        parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
-            try:
-                return float(parts[1])
-            except ValueError:
-                return None
-    return None
+        if line.startswith("#") or ":" not in line:
+            continue
+        k, v = line.split(":", 1)
+        rec[k.strip()] = v.strip()
+    if rec.get("kernel") != kernel:
+        return None, f"the committed record is of {rec.get('kernel')}, not {kernel}"
+    src = "profiles/scan_kernel_dram_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum of " \
+          "bench.py --traffic-case, scaled by pixel-slice-steps)"
+    if rec.get("sources_sha256") != _sources_sha256():
+        return None, src + ": taken on other library sources than this build, not used"
+    return float(rec["bytes_per_pixel_slice_step"]) * pixel_slice_steps, src
 
 
 def _plain(classes, args):
@@ -758,53 +828,89 @@ def _err_vs_fp64(classes, classes_host):
     return {"err_vs_fp64": errs}
 
 
-def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None, from_atoms=False):
-    """The headline workload through simulate_fresnel_as from pinned host
-    buffers; with ``max_angle`` (mrad) the patterns come back cropped to that
-    detector window (the crop fused into the last column pass); with
-    ``from_atoms`` each step uploads the atom lists instead of the potential
-    and builds the potential on the device (gaussian_potential)."""
+def _shard_class(w, rank, world):
+    """This rank's contiguous block of a grid class's probes (strong scaling)."""
+    import dataclasses
+    from wideanglepropagation_b200.distributed import shard_bounds
+    lo, hi = shard_bounds(w.n_probes, rank, world)
+    return dataclasses.replace(w, positions=w.positions[lo:hi], draw_of_probe=w.draw_of_probe[lo:hi])
+
+
+def _positions_of(w):
+    """Pattern index of each probe: its scan position (draw-major probe order);
+    None for a class with one draw (one probe per position already)."""
+    D = w.potential.shape[0]
+    if D == 1:
+        return None
+    P = w.n_probes // D
+    return np.arange(w.n_probes) % P
+
+
+def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, rank=0, max_angle=None, from_atoms=False,
+         accumulate=True):
+    """The headline workload through the public API from pinned host buffers
+    (sharded_simulate_fresnel_as: at one GPU simply simulate_fresnel_as), the
+    draws of each position summed into one pattern (``accumulate``); with
+    ``max_angle`` (mrad) the patterns come back cropped to that detector
+    window (the crop fused into the last column pass); with ``from_atoms``
+    each step uploads the atom lists instead of the potential and builds the
+    potential and the probe on the device (gaussian_potential,
+    aperture_probe)."""
     import torch
+    import torch.distributed as dist
     import wideanglepropagation_b200 as wap
     import wideanglepropagation_b200.synthetic as S
+    from wideanglepropagation_b200.distributed import probe_shard, sharded_simulate_fresnel_as
     host = []
     atoms = []
+    h2d = d2h = 0
     for ci, w in enumerate(classes_host):
         V = torch.from_numpy(w.potential).pin_memory()
+        acc = _positions_of(w) if accumulate else None
+        mine, first, count = probe_shard(w.n_probes, rank, world, acc)
         if from_atoms:
             D, N = w.potential.shape[:2]
             side = int(round((w.n_probes // D) ** 0.5))
             pos, rows = S.batched_scan_class_atoms(ci, w.ny, N, side, D)   # the seeds of batched_scan(0)
             atoms.append((pos, rows, D, N))
+            h2d += pos.nbytes // 2 * 3 + (N * D + 1) * 4                   # (M, 3) float64 + offsets
+        else:
+            h2d += V.numel() * 4 + w.probe.size * 8
         H = wap.angular_spectrum_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
         win = wap.detector_window((w.ny, w.nx), (w.ps, w.ps), w.energy, max_angle) if max_angle else None
-        shape = (w.n_probes, win[2], win[3]) if win else (w.n_probes, w.ny, w.nx)
-        host.append((w, V, torch.from_numpy(w.probe).pin_memory(), torch.from_numpy(w.positions).pin_memory(),
-                     torch.from_numpy(w.draw_of_probe).pin_memory(), H,
-                     torch.empty(shape, dtype=torch.float32).pin_memory()))
-    if from_atoms:
-        h2d = sum(p.nbytes // 2 * 3 + (N * D + 1) * 4 for p, _, D, N in atoms)   # (M, 3) float64 + offsets
-        h2d += sum(p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, _, p, q, d, _, _ in host)
-    else:
-        h2d = sum(V.numel() * 4 + p.numel() * 8 + q.numel() * 4 + d.numel() * 4 for _, V, p, q, d, _, _ in host)
-    d2h = sum(o.numel() * 4 for *_, o in host)
+        shape = (count, win[2], win[3]) if win else (count, w.ny, w.nx)
+        q = torch.from_numpy(w.positions).pin_memory()
+        d = torch.from_numpy(w.draw_of_probe).pin_memory()
+        h2d += len(mine) * (8 + 4) + (len(mine) + count + 1) * 4 * (1 if accumulate else 0)
+        out = torch.empty(shape, dtype=torch.float32).pin_memory()
+        d2h += out.numel() * 4
+        host.append((w, V, torch.from_numpy(w.probe).pin_memory(), q, d, H, out, acc))
+    if world > 1:
+        t = torch.tensor([h2d, d2h], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        h2d, d2h = int(t[0]), int(t[1])
     # patterns go back on a second stream, so that a class's download overlaps
     # the next class's multislice (the end of the timed region waits for it)
     down = torch.cuda.Stream()
 
     def step():
-        for i, (w, V, p, q, d, H, out) in enumerate(host):
+        for i, (w, V, p, q, d, H, out, acc) in enumerate(host):
             if from_atoms:
                 pos, rows, D, N = atoms[i]
                 V = wap.gaussian_potential(D * N, w.ny, w.nx, w.ps, pos, rows, 25.0, 0.25,
                                            scale=1 / w.dz).view(D, N, w.ny, w.nx)
-            _, dp, _ = wap.simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, return_wavefronts=False,
-                                               max_angle=max_angle, sampling=(w.ps, w.ps))
+                p = wap.aperture_probe(w.ny, w.nx, w.ps, w.energy, 25.0, -50.0)
+            # check=False: the scheduler's status is read once per step below,
+            # so the host does not wait for one class before queueing the next
+            dp, _, _ = sharded_simulate_fresnel_as(V, p, H, w.dz, w.energy, positions=q, draw=d, accumulate=acc,
+                                                   gather=False, max_angle=max_angle, sampling=(w.ps, w.ps),
+                                                   check=False)
             down.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(down):
                 out.copy_(dp, non_blocking=True)
             dp.record_stream(down)
         torch.cuda.current_stream().wait_stream(down)
+        wap.check_errors()   # raises if a bounded device-side wait expired
 
     for _ in range(max(1, args.warmup)):
         step()
@@ -818,11 +924,15 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, max_angle=None
     torch.cuda.synchronize()
     ms = max_over_ranks(s.elapsed_time(e)) / args.steps
     total = sum(w.n_probes * w.n_slices for w in classes_host)
-    api = "simulate_fresnel_as(positions=, draw=)" if not max_angle else \
-        f"simulate_fresnel_as(positions=, draw=, max_angle={max_angle:g}, sampling=)"
+    api = "simulate_fresnel_as(positions=, draw=, accumulate=per position)" if accumulate else \
+        "simulate_fresnel_as(positions=, draw=)"
+    if max_angle:
+        api = api[:-1] + f", max_angle={max_angle:g}, sampling=)"
+    if world > 1:
+        api = "sharded_simulate_fresnel_as over " + api
     if from_atoms:
-        api = "gaussian_potential(atoms) + " + api
-    return {"value": total * world / (ms / 1e3), "unit": "slice-steps/s", "h2d_bytes_per_step": h2d,
+        api = "gaussian_potential(atoms) + aperture_probe + " + api
+    return {"value": total / (ms / 1e3), "unit": "slice-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": api}
 
 

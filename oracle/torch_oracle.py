@@ -16,13 +16,17 @@ import torch
 from .propagation_oracle import electron_rest_energy, energy2wavelength
 
 
-def simulate(V, probe, H, dz, energy, positions=None):
+def simulate(V, probe, H, dz, energy, positions=None, device=None):
     """V: (N, ny, nx) float64 tensor (may require grad); probe (ny, nx) complex;
-    returns (exit (B, ny, nx), dp (B, ny, nx))."""
+    returns (exit (B, ny, nx), dp (B, ny, nx)).  Runs on V's device (or
+    ``device`` when V is not a tensor); float64 / complex128 throughout."""
     lam = energy2wavelength(energy)
     E0 = electron_rest_energy()
-    H = torch.as_tensor(H, dtype=torch.complex128)
-    p = torch.as_tensor(probe, dtype=torch.complex128)
+    if not isinstance(V, torch.Tensor):
+        V = torch.as_tensor(np.asarray(V, dtype=np.float64), device=device)
+    dev = V.device
+    H = torch.as_tensor(H).to(dev, torch.complex128)
+    p = torch.as_tensor(probe).to(dev, torch.complex128)
     ny, nx = p.shape[-2:]
     if positions is None:
         waves = p[None] if p.ndim == 2 else p

@@ -22,7 +22,9 @@ It then loads the reference file read-only from the reference checkout, runs
 the path functions on small seeded float64/complex128 inputs (the notebooks
 run with ``jax_enable_x64``) and on float32/complex64 inputs, and writes
 ``tests/golden/golden.npz``.  Re-run with
-``python tests/golden/make_golden.py [path/to/reference]``.
+``python tests/golden/make_golden.py path/to/reference`` (the checkout of
+WideAnglePropagation), or with the path in the environment variable
+``WAP_REFERENCE_ROOT``.
 """
 from __future__ import annotations
 
@@ -35,7 +37,6 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REF = "/root/reference"
 
 
 def _install_stubs():
@@ -294,5 +295,7 @@ def make(ref_root: str, out: str):
 
 
 if __name__ == "__main__":
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_REF
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WAP_REFERENCE_ROOT")
+    if not ref_root:
+        sys.exit("usage: make_golden.py path/to/reference (or set WAP_REFERENCE_ROOT)")
     make(ref_root, os.path.join(HERE, "golden.npz"))

@@ -127,3 +127,34 @@ def test_lippmann_schwinger(golden):
     E, ps, tol = golden["ls_solve_meta"]
     psi = O.solve_scattering_2d_lippmann_schwinger(golden["ls_V"], E, ps, gmres_tol=tol)
     assert O.rel_l2(psi, golden["ls_psi"]) < 1e-10
+
+
+@pytest.mark.parametrize("case", ["fres", "as"])
+def test_torch_gradient_oracle_pinned(golden, case):
+    """The complex128 torch restatement behind the gradient tests reproduces
+    the reference's own Fresnel and (non-square) angular-spectrum outputs."""
+    import torch
+    from oracle import torch_oracle as T
+    ny, nx, ps, N, dz, E = golden[f"{case}_meta"]
+    ex, dp = T.simulate(torch.tensor(golden[f"{case}_V"], dtype=torch.float64), golden[f"{case}_probe"],
+                        golden[f"{case}_H"], dz, E)
+    close(ex[0].numpy(), golden[f"{case}_exit"])
+    close(dp[0].numpy(), golden[f"{case}_dp"])
+
+
+def test_torch_gradient_oracle_positions():
+    """With probe positions the torch restatement matches the NumPy oracle's
+    move_probe (pinned to the reference's roll above) probe for probe."""
+    import torch
+    from oracle import torch_oracle as T
+    rng = np.random.default_rng(3)
+    n, N, dz, E = 32, 3, 2.0, 300e3
+    V = rng.uniform(0, 30, (N, n, n))
+    probe = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    H = O.fresnel_propagation_kernel(n, n, (0.1, 0.1), dz, E)
+    pos = np.array([[3, 30], [16, 16], [31, 0]])
+    ex, dp = T.simulate(torch.tensor(V), probe, H, dz, E, pos)
+    for b, p in enumerate(pos):
+        rex, rdp, _ = O.simulate_fresnel_as(V, O.move_probe(probe, tuple(p)), H, dz, E, return_wavefronts=False)
+        close(ex[b].numpy(), rex)
+        close(dp[b].numpy(), rdp)

@@ -396,6 +396,7 @@ int wap_plan_destroy(wap_plan* p) {
   cudaFree(p->kx2);
   cudaFree(p->refs);
   cudaFree(p->ttab);
+  cudaFree(p->counter);
   delete p;
   return WAP_OK;
 }

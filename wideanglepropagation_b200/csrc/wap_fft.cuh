@@ -89,8 +89,28 @@ __host__ __device__ inline PlanShape make_plan_shape(int n, int e) {
 // ----------------------------------------------------------------------------
 // complex helpers
 // ----------------------------------------------------------------------------
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add / subtract as one packed FP32x2 instruction (sm_100 add/sub
+// .f32x2: both lanes rounded exactly like two scalar adds), halving the issue
+// slots of the butterflies' additions.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+// a + (-i) b and a - (-i) b (forward sign; INV: +i), the rotated pair of a
+// radix-4 butterfly: scalar adds, since the rotation swaps the lanes
+template <bool INV>
+__device__ __forceinline__ float2 cadd_rot(float2 a, float2 b) {
+  return INV ? make_float2(a.x - b.y, a.y + b.x) : make_float2(a.x + b.y, a.y - b.x);
+}
+template <bool INV>
+__device__ __forceinline__ float2 csub_rot(float2 a, float2 b) {
+  return INV ? make_float2(a.x + b.y, a.y - b.x) : make_float2(a.x - b.y, a.y + b.x);
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
@@ -203,11 +223,23 @@ __device__ __forceinline__ void dft2(float2& a0, float2& a1) {
 template <bool INV>
 __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
   float2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
-  float2 t2 = cadd(a1, a3), t3 = mul_mi<INV>(csub(a1, a3));
+  float2 t2 = cadd(a1, a3), d = csub(a1, a3);
   a0 = cadd(t0, t2);
   a2 = csub(t0, t2);
-  a1 = cadd(t1, t3);
-  a3 = csub(t1, t3);
+  a1 = cadd_rot<INV>(t1, d);   // t1 + (-+i) d
+  a3 = csub_rot<INV>(t1, d);
+}
+
+// dft4 whose input a2 still carries a factor -+i (W16^4 of the radix-16
+// codelet): the rotation is folded into the additions that use a2
+template <bool INV>
+__device__ __forceinline__ void dft4_rot2(float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 t0 = cadd_rot<INV>(a0, a2), t1 = csub_rot<INV>(a0, a2);
+  float2 t2 = cadd(a1, a3), d = csub(a1, a3);
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd_rot<INV>(t1, d);
+  a3 = csub_rot<INV>(t1, d);
 }
 
 template <int R, bool INV>
@@ -221,15 +253,20 @@ __device__ __forceinline__ void dft(float2 (&a)[R]) {
     // n = n1 + 2 n2, k = 4 k1 + k2
 #pragma unroll
     for (int n1 = 0; n1 < 2; ++n1) dft4<INV>(a[n1], a[n1 + 2], a[n1 + 4], a[n1 + 6]);
-    // Y[n1][k2] sits in a[n1 + 2 k2]
-#pragma unroll
-    for (int k2 = 1; k2 < 4; ++k2) a[1 + 2 * k2] = tw16<INV>(a[1 + 2 * k2], 2 * k2);
+    // Y[n1][k2] sits in a[n1 + 2 k2]; W16^4 (k2 = 2) is folded into its additions
+    a[3] = tw16<INV>(a[3], 2);
+    a[7] = tw16<INV>(a[7], 6);
     float2 o[8];
 #pragma unroll
     for (int k2 = 0; k2 < 4; ++k2) {
       float2 y0 = a[2 * k2], y1 = a[1 + 2 * k2];
-      o[k2] = cadd(y0, y1);
-      o[4 + k2] = csub(y0, y1);
+      if (k2 == 2) {
+        o[k2] = cadd_rot<INV>(y0, y1);
+        o[4 + k2] = csub_rot<INV>(y0, y1);
+      } else {
+        o[k2] = cadd(y0, y1);
+        o[4 + k2] = csub(y0, y1);
+      }
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) a[i] = o[i];
@@ -237,16 +274,19 @@ __device__ __forceinline__ void dft(float2 (&a)[R]) {
     // n = n1 + 4 n2, k = 4 k1 + k2
 #pragma unroll
     for (int n1 = 0; n1 < 4; ++n1) dft4<INV>(a[n1], a[n1 + 4], a[n1 + 8], a[n1 + 12]);
-    // Y[n1][k2] sits in a[n1 + 4 k2]
+    // Y[n1][k2] sits in a[n1 + 4 k2]; W16^4 (n1 = k2 = 2) is folded into the
+    // additions of its dft4
 #pragma unroll
     for (int n1 = 1; n1 < 4; ++n1)
 #pragma unroll
-      for (int k2 = 1; k2 < 4; ++k2) a[n1 + 4 * k2] = tw16<INV>(a[n1 + 4 * k2], n1 * k2);
+      for (int k2 = 1; k2 < 4; ++k2)
+        if (n1 * k2 != 4) a[n1 + 4 * k2] = tw16<INV>(a[n1 + 4 * k2], n1 * k2);
     float2 o[16];
 #pragma unroll
     for (int k2 = 0; k2 < 4; ++k2) {
       float2 y0 = a[4 * k2], y1 = a[1 + 4 * k2], y2 = a[2 + 4 * k2], y3 = a[3 + 4 * k2];
-      dft4<INV>(y0, y1, y2, y3);
+      if (k2 == 2) dft4_rot2<INV>(y0, y1, y2, y3);
+      else dft4<INV>(y0, y1, y2, y3);
       o[k2] = y0;
       o[4 + k2] = y1;
       o[8 + k2] = y2;

@@ -40,6 +40,7 @@ struct wap_plan {
   float2* ttab = nullptr;                   // transmission table (draws, n_slices, ny, nx)
   size_t ttab_cap = 0;
   wap::Detector det;                        // diffraction-pattern window (wap_plan_set_detector)
+  unsigned long long* counter = nullptr;    // probe builder: aperture pixel count (allocated on first use)
 };
 
 namespace wap {
@@ -73,6 +74,8 @@ cudaError_t launch_wpm_row(int n, int e, const WpmRowArgs& a, int nb, int k, cud
 int wpm_col_occupancy(int n, int e, int k, int K);
 int wpm_row_occupancy(int n, int e, int k, int K);
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
+cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t st);
+ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo);
 RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
 int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st);
 

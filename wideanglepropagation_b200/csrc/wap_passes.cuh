@@ -671,7 +671,7 @@ struct WpmRowArgs {
 };
 
 template <int NX, int E>
-__global__ void __launch_bounds__(kRowThreads)
+__global__ void __launch_bounds__(kRowThreads, E <= 8 ? 3 : 1)
 wpm_row_kernel(const WpmRowArgs a) {
   using C = RowCfg<NX, E>;
   constexpr int T = C::T;
