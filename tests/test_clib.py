@@ -44,7 +44,7 @@ def test_version_and_no_error(lib):
     assert lib.wap_last_error() == b""
 
 
-@pytest.mark.parametrize("ny,nx", [(100, 128), (128, 96), (16, 64), (4096, 64), (0, 64)])
+@pytest.mark.parametrize("ny,nx", [(16, 64), (4096, 64), (0, 64), (1025, 128), (128, 2000), (64, 12)])
 def test_unsupported_grid(lib, ny, nx):
     from wideanglepropagation_b200 import _lib
     h = ctypes.c_void_p()
@@ -52,6 +52,19 @@ def test_unsupported_grid(lib, ny, nx):
     assert rc == _lib.WAP_ERR_UNSUPPORTED
     assert b"unsupported grid" in lib.wap_last_error()
     assert not h.value
+
+
+@pytest.mark.parametrize("ny,nx", [(100, 128), (128, 96), (17, 1024), (1000, 2048)])
+def test_generic_grids_pass_the_size_check(lib, ny, nx):
+    """Sides that are not powers of two (17 .. 1024) take the Bluestein path:
+    the size check accepts them (without a device the plan then fails on its
+    first CUDA call, never as an unsupported size)."""
+    from wideanglepropagation_b200 import _lib
+    h = ctypes.c_void_p()
+    rc = lib.wap_plan_create(ctypes.byref(h), ny, nx, 1, 0, 0)
+    assert rc != _lib.WAP_ERR_UNSUPPORTED
+    if rc == _lib.WAP_OK:
+        lib.wap_plan_destroy(h)
 
 
 def test_bad_arguments(lib):
@@ -74,7 +87,7 @@ def test_check_maps_codes_to_exceptions(lib):
     from wideanglepropagation_b200 import _lib
     h = ctypes.c_void_p()
     with pytest.raises(ValueError, match="unsupported grid"):
-        _lib.check(lib.wap_plan_create(ctypes.byref(h), 100, 100, 1, 0, 0))
+        _lib.check(lib.wap_plan_create(ctypes.byref(h), 100, 2000, 1, 0, 0))
 
 
 def test_launch_counter_starts_at_zero(lib):

@@ -333,6 +333,27 @@ static bool config_valid(const wap_plan* p, int row_e, int col_e, int col_w) {
   return true;
 }
 
+static void plan_free(wap_plan* p) {
+  if (!p) return;
+  cudaFree(p->tw_row);
+  cudaFree(p->tw_col);
+  cudaFree(p->fields);
+  cudaFree(p->dpbuf);
+  cudaFree(p->blend);
+  cudaFree(p->hvac);
+  cudaFree(p->hvac_lo);
+  cudaFree(p->ky2);
+  cudaFree(p->kx2);
+  cudaFree(p->refs);
+  cudaFree(p->ttab);
+  cudaFree(p->counter);
+  if (p->generic) {
+    generic_axis_free(&p->gen_x);
+    generic_axis_free(&p->gen_y);
+  }
+  delete p;
+}
+
 extern "C" {
 
 const char* wap_version(void) { return "wap-b200 0.1 (sm_100a)"; }
@@ -343,8 +364,14 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
   clear_error();
   if (!out) return fail(WAP_ERR_ARG, "plan pointer is NULL");
   *out = nullptr;
-  if (!size_supported(ny) || !size_supported(nx))
-    return fail(WAP_ERR_UNSUPPORTED, "unsupported grid %d x %d: each axis must be a power of two in [32, 2048]", ny, nx);
+  // power-of-two grids in [32, 2048] take the fast path; a grid with another
+  // side (17 .. 1024) runs the Bluestein transforms of wap_generic.cu
+  const bool generic = !size_supported(ny) || !size_supported(nx);
+  auto axis_ok = [](int n) { return size_supported(n) || generic_size_supported(n); };
+  if (!axis_ok(ny) || !axis_ok(nx))
+    return fail(WAP_ERR_UNSUPPORTED,
+                "unsupported grid %d x %d: each axis must be a power of two in [32, 2048] or a size in [17, 1024]", ny,
+                nx);
   if (max_batch < 1) return fail(WAP_ERR_ARG, "max_batch must be >= 1 (got %d)", max_batch);
   if (op != WAP_OP_FRESNEL_AS && op != WAP_OP_WPM) return fail(WAP_ERR_ARG, "unknown op %d", op);
   if (op == WAP_OP_WPM && (n_bins < 2 || n_bins > 4096))
@@ -359,9 +386,11 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
   p->row_e = nx >= 64 ? 16 : 8;
   p->col_e = ny >= 64 ? 16 : 8;
   p->col_w = default_col_w(ny, p->col_e, nx);
-  int rc = upload_twiddles(p);
+  p->generic = generic;
+  int rc = generic ? generic_axis_create(&p->gen_x, nx) : upload_twiddles(p);
+  if (rc == WAP_OK && generic) rc = generic_axis_create(&p->gen_y, ny);
   if (rc != WAP_OK) {
-    wap_plan_destroy(p);
+    plan_free(p);   // keeps the failure's message
     return rc;
   }
   if (op == WAP_OP_WPM) {
@@ -374,7 +403,7 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
     if (err == cudaSuccess) err = cudaMalloc(&p->ky2, ny * sizeof(float));
     if (err == cudaSuccess) err = cudaMalloc(&p->kx2, nx * sizeof(float));
     if (err != cudaSuccess) {
-      wap_plan_destroy(p);
+      plan_free(p);
       return cuda_fail(err, "cudaMalloc(WPM workspace)");
     }
   }
@@ -384,26 +413,14 @@ int wap_plan_create(wap_plan** out, int ny, int nx, int max_batch, int op, int n
 
 int wap_plan_destroy(wap_plan* p) {
   clear_error();
-  if (!p) return WAP_OK;
-  cudaFree(p->tw_row);
-  cudaFree(p->tw_col);
-  cudaFree(p->fields);
-  cudaFree(p->dpbuf);
-  cudaFree(p->blend);
-  cudaFree(p->hvac);
-  cudaFree(p->hvac_lo);
-  cudaFree(p->ky2);
-  cudaFree(p->kx2);
-  cudaFree(p->refs);
-  cudaFree(p->ttab);
-  cudaFree(p->counter);
-  delete p;
+  plan_free(p);
   return WAP_OK;
 }
 
 int wap_plan_set_config(wap_plan* p, int row_e, int col_e, int col_w) {
   clear_error();
   if (!p) return fail(WAP_ERR_ARG, "plan is NULL");
+  if (p->generic) return fail(WAP_ERR_UNSUPPORTED, "grids that are not powers of two have a fixed launch shape");
   if (!config_valid(p, row_e, col_e, col_w))
     return fail(WAP_ERR_ARG, "invalid launch configuration row_e=%d col_e=%d col_w=%d for %d x %d", row_e, col_e, col_w,
                 p->ny, p->nx);
@@ -488,6 +505,7 @@ RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int 
   r.ri_inv_den = (float)ph.ri_inv_den;
   r.kphase = (float)ph.kphase;
   r.e_plus_e0 = (float)ph.e_plus_e0;
+  r.tw_ready = 1;   // uploaded at plan creation
   return r;
 }
 
@@ -500,6 +518,7 @@ ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo) {
   c.nx = p->nx;
   c.seed_scale = (float)((double)p->ny * p->nx);
   c.det = p->det.resolved(p->ny, p->nx);
+  c.tw_ready = 1;
   return c;
 }
 
@@ -595,6 +614,13 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   if (rc) return rc;
   if (!H) return fail(WAP_ERR_ARG, "H must be a non-NULL device pointer");
   if (p->op != WAP_OP_FRESNEL_AS) return fail(WAP_ERR_ARG, "plan was not created for the Fresnel/AS path");
+  if (p->generic) {
+    if (ckpt)
+      return fail(WAP_ERR_UNSUPPORTED, "checkpointed forwards (gradients) need power-of-two grids, got %d x %d", p->ny,
+                  p->nx);
+    return generic_fresnel_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, H, H_lo,
+                                   dz, energy, exit, dp, stack, st);
+  }
   const Physics ph = physics(energy, dz);
   const long long plane = (long long)p->ny * p->nx;
   const int nck = ckpt ? (n_slices + ckpt_every - 1) / ckpt_every : 0;
@@ -649,6 +675,7 @@ int wap_spectrum_propagate(wap_plan* p, const float* X, int n, const float* H, c
   clear_error();
   if (!p || !X || !H || !out) return fail(WAP_ERR_ARG, "NULL argument");
   if (n < 1 || n > p->max_batch) return fail(WAP_ERR_ARG, "n=%d outside 1..%d (plan batch)", n, p->max_batch);
+  if (p->generic) return fail(WAP_ERR_UNSUPPORTED, "spectrum propagation needs a power-of-two grid");
   cudaStream_t st = (cudaStream_t)stream;
   const long long plane = (long long)p->ny * p->nx;
   cudaError_t e;
@@ -670,6 +697,7 @@ int wap_spectrum_propagate(wap_plan* p, const float* X, int n, const float* H, c
   r.nx = p->nx;
   r.flags = ROW_IFFT;
   r.scale = (float)(1.0 / (double)plane);
+  r.tw_ready = 1;
   if ((e = row_chunks(p, r, n, st)) != cudaSuccess) return cuda_fail(e, "spectrum row pass");
   return WAP_OK;
 }
@@ -707,6 +735,7 @@ int wap_multislice_bwd(wap_plan* p, const float* V, int n_slices, int n_draws, c
   if (!grad_dp && !grad_exit) return fail(WAP_ERR_ARG, "need grad_dp or grad_exit");
   if (ckpt_every < 1) return fail(WAP_ERR_ARG, "ckpt_every must be >= 1");
   if (p->op != WAP_OP_FRESNEL_AS) return fail(WAP_ERR_ARG, "plan was not created for the Fresnel/AS path");
+  if (p->generic) return fail(WAP_ERR_UNSUPPORTED, "gradients need power-of-two grids, got %d x %d", p->ny, p->nx);
   cudaStream_t st = (cudaStream_t)stream;
   const Physics ph = physics(energy, dz);
   const long long plane = (long long)p->ny * p->nx;

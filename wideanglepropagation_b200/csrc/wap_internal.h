@@ -18,6 +18,19 @@ struct Detector {
   // pixels of one probe's pattern
   __host__ __device__ long long plane() const { return (long long)ny * nx; }
 };
+
+// One axis of a grid that is not a power of two (wap_generic.cu): a length-n
+// DFT as Bluestein's chirp convolution through an m-point FFT (m the power of
+// two >= 2n - 1), or, for a power-of-two axis of such a grid, the plain
+// n-point FFT (m = n, blue = 0).  Device pointers; tables of float64 values
+// stored as float hi + lo parts.
+struct GenAxis {
+  int n = 0, m = 0, e = 16, blue = 0;
+  const float4* tw = nullptr;       // twiddles of the m-point FFT
+  const float4* chirp = nullptr;    // (n) w_p = exp(-i pi p^2 / n)
+  const float4* bhat_f = nullptr;   // (m) fft_m(b) / m, b_q = conj(w_q) on the circular index range
+  const float4* bhat_i = nullptr;   // (m) fft_m(conj(b)) / m
+};
 }  // namespace wap
 
 struct wap_plan {
@@ -41,6 +54,9 @@ struct wap_plan {
   size_t ttab_cap = 0;
   wap::Detector det;                        // diffraction-pattern window (wap_plan_set_detector)
   unsigned long long* counter = nullptr;    // probe builder: aperture pixel count (allocated on first use)
+  // a grid with an axis that is not a power of two: Bluestein transforms
+  bool generic = false;
+  wap::GenAxis gen_x, gen_y;                // along x (rows) and y (columns)
 };
 
 namespace wap {
@@ -75,6 +91,19 @@ int wpm_col_occupancy(int n, int e, int k, int K);
 int wpm_row_occupancy(int n, int e, int k, int K);
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
 cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t st);
+
+// grids that are not powers of two (wap_generic.cu)
+bool generic_size_supported(int n);
+int generic_axis_create(GenAxis* ax, int n);
+void generic_axis_free(GenAxis* ax);
+int generic_fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw,
+                            const float* psi0, int n_probes, int psi0_per_probe, const int32_t* positions,
+                            const float* H, const float* H_lo, double dz, double energy, float* exit, float* dp,
+                            float* stack, cudaStream_t st);
+int generic_wpm_forward(wap_plan* p, const float* V, int n_slices, int n_draws, const int32_t* draw,
+                        const float* psi0, int n_probes, int psi0_per_probe, const int32_t* positions, double dz,
+                        double energy, double sampling_y, double sampling_x, double power_spacing, float* exit,
+                        float* dp, float* stack, cudaStream_t st);
 ColArgs base_col_args(const wap_plan* p, const float* H, const float* H_lo);
 RowArgs base_row_args(const wap_plan* p, const Physics& ph, const float* V, int n_slices, const int32_t* draw);
 int build_trans_table(wap_plan* p, const float* V, int n_slices, int n_draws, const RowArgs& r, cudaStream_t st);

@@ -78,6 +78,8 @@ struct RowArgs {
   float ri_a, ri_inv_den;    // n^2 - 1 = V (a + V) inv_den
   float kphase;              // 2 pi dz / lambda
   float e_plus_e0;           // E + E0 (for dn/dV)
+  int tw_ready;              // tw was not written by a kernel of this stream (a plan's
+                             // table): read before the programmatic-launch wait
 };
 
 struct ColArgs {
@@ -95,6 +97,7 @@ struct ColArgs {
   int flags;
   int probe0;
   float seed_scale;          // n_px
+  int tw_ready;              // as RowArgs::tw_ready
 };
 
 // numpy.fft.fftfreq(n, d)[i] in float64: i * (1/(n d)) with the upper half
@@ -182,8 +185,13 @@ row_pass_kernel(const RowArgs a) {
   extern __shared__ float4 smem_raw[];
   float4* tw = smem_raw;
   float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
+  // a plan's twiddles do not depend on the previous pass: their load overlaps
+  // its tail (one L2 round trip less on the chain of a single probe)
+  if (a.tw_ready)
+    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
   pdl_wait_then_release();
-  for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
+  if (!a.tw_ready)
+    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
   const int rl = threadIdx.x / T;
@@ -219,6 +227,17 @@ row_pass_kernel(const RowArgs a) {
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = __ldcg(prow + t + T * e);
   }
+  // Short-chain shapes (E <= 8, the single-probe launches) fetch the
+  // transmission row before the inverse transform, so its L2 latency overlaps
+  // the transform instead of following it; E = 16 keeps the registers.
+  constexpr bool kEarlyT = E <= 8;
+  float2 tpre[kEarlyT ? E : 1];
+  if (kEarlyT && (f & ROW_TRANS_TAB)) {
+    const int d = a.draw ? a.draw[b] : 0;
+    const float2* trow = a.ttab + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
+#pragma unroll
+    for (int e = 0; e < (kEarlyT ? E : 1); ++e) tpre[e] = __ldg(trow + t + T * e);
+  }
 
   if (f & ROW_IFFT) {
     fft<NX, E, true>(v, t, xs, tw);
@@ -233,10 +252,15 @@ row_pass_kernel(const RowArgs a) {
   }
 
   if (f & ROW_TRANS_TAB) {
-    const int d = a.draw ? a.draw[b] : 0;
-    const float2* trow = a.ttab + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
+    if constexpr (kEarlyT) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
+      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], tpre[e]);
+    } else {
+      const int d = a.draw ? a.draw[b] : 0;
+      const float2* trow = a.ttab + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(trow + t + T * e));
+    }
   } else if (f & (ROW_TRANS | ROW_ADJOINT)) {
     const int d = a.draw ? a.draw[b] : 0;
     const float* vrow = a.V + (long long)d * a.v_draw_stride + (long long)a.slice * plane + (long long)row * NX;
@@ -322,8 +346,11 @@ col_pass_kernel(const ColArgs a) {
   extern __shared__ float4 smem_raw[];
   float4* tw = smem_raw;
   float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
+  if (a.tw_ready)
+    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
   pdl_wait_then_release();
-  for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
+  if (!a.tw_ready)
+    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
   __syncthreads();
 
   const int c = threadIdx.x % W;
@@ -338,6 +365,18 @@ col_pass_kernel(const ColArgs a) {
 
   float2 v[E];
   tile_load<NY>(tile, ptile, W, nx);
+  // short-chain shapes fetch H (hi and lo) before the forward transform, as
+  // the row pass does with the transmission
+  constexpr bool kEarlyH = E <= 8;
+  float2 hpre[kEarlyH ? E : 1], lpre[kEarlyH ? E : 1];
+  if (kEarlyH && !(f & COL_NO_H)) {
+#pragma unroll
+    for (int e = 0; e < (kEarlyH ? E : 1); ++e) {
+      const long long o = (long long)(t + T * e) * nx + col;
+      hpre[e] = __ldg(a.H + o);
+      lpre[e] = a.H_lo ? __ldg(a.H_lo + o) : make_float2(0.f, 0.f);
+    }
+  }
   __syncthreads();
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
@@ -371,7 +410,15 @@ col_pass_kernel(const ColArgs a) {
     }
   }
 
-  if (!(f & COL_NO_H)) {
+  if (kEarlyH && !(f & COL_NO_H)) {
+    if (f & COL_CONJ_H) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cmulc_hl(v[e], hpre[e], lpre[e]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cmul_hl(v[e], hpre[e], lpre[e]);
+    }
+  } else if (!(f & COL_NO_H)) {
     const float2* hcol = a.H + col;
     if (a.H_lo) {
       const float2* lcol = a.H_lo + col;

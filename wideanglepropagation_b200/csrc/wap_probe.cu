@@ -121,6 +121,7 @@ int wap_aperture_probe(wap_plan* p, double ps_y, double ps_x, double energy, dou
   int dev = -1;
   cudaGetDevice(&dev);
   if (dev != p->device) return fail(WAP_ERR_ARG, "plan was created on device %d, current device is %d", p->device, dev);
+  if (p->generic) return fail(WAP_ERR_UNSUPPORTED, "the probe builder needs a power-of-two grid");
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
   if (!p->counter && (e = cudaMalloc(&p->counter, sizeof(unsigned long long))) != cudaSuccess)
@@ -149,6 +150,7 @@ int wap_aperture_probe(wap_plan* p, double ps_y, double ps_x, double energy, dou
   r.nx = p->nx;
   r.flags = ROW_IFFT;
   r.scale = 1.0f;
+  r.tw_ready = 1;
   if ((e = row_chunks(p, r, 1, st)) != cudaSuccess) return cuda_fail(e, "probe row pass");
   count_launch();
   probe_normalise_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<float2*>(out), total, p->counter);

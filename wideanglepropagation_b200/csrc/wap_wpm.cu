@@ -87,6 +87,9 @@ extern "C" int wap_wpm_fwd(wap_plan* p, const float* V, int n_slices, int n_draw
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "wpm_vacuum_kernel");
     std::copy(key, key + 4, p->hvac_key);
   }
+  if (p->generic)
+    return generic_wpm_forward(p, V, n_slices, n_draws, draw, psi0, n_probes, psi0_per_probe, positions, dz, energy,
+                               sampling_y, sampling_x, power_spacing, exit, dp, stack, st);
 
   WpmBinsArgs bargs{V, p->refs, (int)plane, n_slices, K, (float)ph.ri_a, (float)ph.ri_inv_den, power_spacing};
   {

@@ -36,6 +36,13 @@ def shard(seq, rank: int, world: int):
     return seq[lo:hi]
 
 
+def _pinned(a: np.ndarray) -> torch.Tensor:
+    """A host array as a pinned tensor (uploads without waiting for the queued
+    work); plain CPU memory where no CUDA device is present (the CPU tests)."""
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.pin_memory() if torch.cuda.is_available() else t
+
+
 def _rank_world(group) -> tuple:
     if dist.is_available() and dist.is_initialized():
         return dist.get_rank(group), dist.get_world_size(group)
@@ -115,15 +122,18 @@ def sharded_simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, 
     pos = np.asarray(positions.cpu() if isinstance(positions, torch.Tensor) else positions).reshape(-1, 2)
     B = pos.shape[0]
     mine, first, count = probe_shard(B, rank, world, accumulate)
+    whole = len(mine) == B   # one rank (or all probes here): pass the caller's arrays through unchanged
+    local_pos = positions if whole else _pinned(pos[mine])
     dr = None
     if draw is not None:
-        dr = np.asarray(draw.cpu() if isinstance(draw, torch.Tensor) else draw).reshape(-1)[mine]
+        dr = draw if whole else _pinned(np.asarray(draw.cpu() if isinstance(draw, torch.Tensor) else draw)
+                                        .reshape(-1)[mine])
     acc_local = None
     if accumulate is not None:
         acc = np.asarray(accumulate.cpu() if isinstance(accumulate, torch.Tensor) else accumulate).reshape(-1)
         acc_local = acc[mine] - first
     if len(mine):
-        ex, dp, _ = forward(potential, probe, prop_kernel, slice_thickness, energy, positions=pos[mine],
+        ex, dp, _ = forward(potential, probe, prop_kernel, slice_thickness, energy, positions=local_pos,
                             draw=dr, accumulate=acc_local, return_wavefronts=False, **kwargs)
         if accumulate is not None and dp.shape[0] < count:
             # trailing patterns of this block that no probe maps to

@@ -410,6 +410,14 @@ def _detector(shape, sampling, energy, max_angle, parity):
     return detector_window(shape, _pair(sampling), energy, max_angle, parity)
 
 
+def _upload_small(a: np.ndarray, dev) -> torch.Tensor:
+    """A small host array on the device through pinned memory and a
+    non-blocking copy: a pageable copy may wait for the work already queued on
+    the stream (e.g. a whole scan) before it returns."""
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return _to(t.pin_memory(), t.dtype, dev)
+
+
 def _dp_shape(B, ny, nx, det):
     return (B, det[2], det[3]) if det is not None else (B, ny, nx)
 
@@ -429,7 +437,7 @@ def _accumulation(accumulate, B, dev):
     P = int(idx.max()) + 1 if idx.size else 0
     order = np.argsort(idx, kind="stable").astype(np.int32)
     start = np.concatenate([[0], np.cumsum(np.bincount(idx, minlength=P))]).astype(np.int32)
-    return P, torch.as_tensor(start).to(dev), torch.as_tensor(order).to(dev)
+    return P, _upload_small(start, dev), _upload_small(order, dev)
 
 
 def accumulate_patterns(dp: torch.Tensor, accumulate) -> torch.Tensor:
