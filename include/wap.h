@@ -40,8 +40,12 @@ const char* wap_version(void);
 /* Message of the calling thread's last failed call ("" if none). */
 const char* wap_last_error(void);
 
-/* Create a plan for ny x nx grids (powers of two, 32..2048 per axis) and up
- * to max_batch probes per call.  op is WAP_OP_*; n_bins is the WPM bin count
+/* Create a plan for ny x nx grids and up to max_batch probes per call.  Sides
+ * that are powers of two in [32, 2048] take the fast kernels; a grid with
+ * another side (any n in [17, 1024]) runs Bluestein transforms through the
+ * same FFT core (wap_multislice_fwd and wap_wpm_fwd only; the checkpointed
+ * forward, the adjoint, wap_spectrum_propagate and wap_aperture_probe return
+ * WAP_ERR_UNSUPPORTED for such plans).  op is WAP_OP_*; n_bins is the WPM bin count
  * (ignored for WAP_OP_FRESNEL_AS).  Allocates twiddle tables and, for WPM,
  * the per-probe reference-field workspace on the current device.
  * Replaces the per-call setup implicit in propagation.py:305 / :358. */
@@ -49,6 +53,13 @@ int wap_plan_create(wap_plan** plan, int ny, int nx, int max_batch, int op, int 
 
 /* Release a plan and everything it allocated. */
 int wap_plan_destroy(wap_plan* plan);
+
+/* Status of the plan's last one-launch chain (single-probe forwards run all
+ * slices in one cooperative kernel whose grid-wide waits are bounded): a copy
+ * of the status word (0 or WAP_ERR_TIMEOUT) into host_status, pinned host
+ * memory, enqueued on `stream`; valid once the stream reaches it.  No
+ * counterpart in the reference. */
+int wap_plan_status_async(wap_plan* plan, int* host_status, void* stream);
 
 /* FFT launch shape of the row pass (elements per thread) and column pass
  * (elements per thread, columns per CTA); set by the autotuner.  Elements
@@ -316,13 +327,16 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *   WAP_KNOB_TW_SMEM   1: twiddles in shared memory, 0: read through L1
  *   WAP_KNOB_PSI       how adjoint rows read psi_s: 0 global, 1 second stage,
  *                      2 the one stage refilled (default)
- *   WAP_KNOB_GROUP     probe-group size of classes that ask for automatic */
+ *   WAP_KNOB_GROUP     probe-group size of classes that ask for automatic
+ *   WAP_KNOB_CHAIN     0: single-probe forwards as one launch per pass instead
+ *                      of the one-launch chain kernel (default 1) */
 #define WAP_KNOB_ELEMS 0
 #define WAP_KNOB_TWIDDLES 1
 #define WAP_KNOB_TW_SMEM 2
 #define WAP_KNOB_PSI 3
 #define WAP_KNOB_GROUP 4
-#define WAP_KNOB_COUNT 5
+#define WAP_KNOB_CHAIN 5
+#define WAP_KNOB_COUNT 6
 #define WAP_TW_FULL 1
 #define WAP_TW_HI 2
 int wap_scan_debug_override(int which, int value);

@@ -24,7 +24,7 @@ WAP_OP_WPM = 1
 WAP_TF_FRESNEL = 0
 WAP_TF_ANGULAR = 1
 
-WAP_KNOB_ELEMS, WAP_KNOB_TWIDDLES, WAP_KNOB_TW_SMEM, WAP_KNOB_PSI, WAP_KNOB_GROUP = range(5)
+WAP_KNOB_ELEMS, WAP_KNOB_TWIDDLES, WAP_KNOB_TW_SMEM, WAP_KNOB_PSI, WAP_KNOB_GROUP, WAP_KNOB_CHAIN = range(6)
 WAP_TW_FULL = 1
 WAP_TW_HI = 2
 
@@ -64,6 +64,7 @@ SIGNATURES = {
     "wap_scan_bind": (_I, [_P, _I, _P]),
     "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
     "wap_scan_status_async": (_I, [_P, _P, _P]),
+    "wap_plan_status_async": (_I, [_P, _P, _P]),
     "wap_scan_debug_override": (_I, [_I, _I]),
     "wap_scan_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_scan_destroy": (_I, [_P]),
@@ -133,14 +134,15 @@ _pending: list = []
 _pending_lock = threading.Lock()
 
 
-def scan_status_begin(handle, what: str):
-    """Enqueue, on the current stream, a copy of a scan's status word into
-    pinned host memory and record an event after it; returns the token that
-    ``scan_status_end`` or ``defer_status`` take."""
+def scan_status_begin(handle, what: str, source: str = "wap_scan_status_async"):
+    """Enqueue, on the current stream, a copy of a scan's (or, with
+    source="wap_plan_status_async", a plan's one-launch chain's) status word
+    into pinned host memory and record an event after it; returns the token
+    that ``scan_status_end`` or ``defer_status`` take."""
     import torch
     word = torch.zeros(1, dtype=torch.int32, pin_memory=True)
     stream = torch.cuda.current_stream()
-    check(lib().wap_scan_status_async(handle, ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
+    check(getattr(lib(), source)(handle, ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
     ev = torch.cuda.Event()
     ev.record(stream)
     return ev, word, what

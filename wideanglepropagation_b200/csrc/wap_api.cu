@@ -347,6 +347,9 @@ static void plan_free(wap_plan* p) {
   cudaFree(p->refs);
   cudaFree(p->ttab);
   cudaFree(p->counter);
+  cudaFree(p->chain_tw);
+  cudaFree(p->chain_count);
+  cudaFree(p->chain_status);
   if (p->generic) {
     generic_axis_free(&p->gen_x);
     generic_axis_free(&p->gen_y);
@@ -644,6 +647,12 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   c.psi = r.psi;
   c.psi_bstride = plane;
   c.dp = dp;
+  // one or two probes: every slice in one cooperative launch when the grid
+  // qualifies (wap_chain.cu), else one launch per pass below
+  if (!ckpt) {
+    const int rc2 = chain_forward(p, r, c, n_probes, n_slices, reinterpret_cast<float2*>(stack), st);
+    if (rc2 != -1) return rc2;
+  }
 
   for (int s = 0; s <= n_slices; ++s) {
     r.slice = s;

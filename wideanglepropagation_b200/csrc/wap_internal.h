@@ -57,6 +57,12 @@ struct wap_plan {
   // a grid with an axis that is not a power of two: Bluestein transforms
   bool generic = false;
   wap::GenAxis gen_x, gen_y;                // along x (rows) and y (columns)
+  // one-launch chain of a single probe (wap_chain.cu): its twiddle table,
+  // grid-barrier counter and status word (allocated on first use)
+  float4* chain_tw = nullptr;
+  int chain_e = 0;
+  unsigned* chain_count = nullptr;
+  int* chain_status = nullptr;
 };
 
 namespace wap {
@@ -91,6 +97,13 @@ int wpm_col_occupancy(int n, int e, int k, int K);
 int wpm_row_occupancy(int n, int e, int k, int K);
 cudaError_t row_chunks(const wap_plan* p, RowArgs r, int n_probes, cudaStream_t st);
 cudaError_t col_chunks(const wap_plan* p, ColArgs c, int n_probes, cudaStream_t st);
+
+// scheduler / chain overrides (wap_scan_debug_override), -1: default
+int knob_value(int which);
+// one-launch chain of a single probe (wap_chain.cu); returns -1 when the
+// plan or the call does not qualify (the caller then launches per pass)
+int chain_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes, int n_slices, float2* stack,
+                  cudaStream_t st);
 
 // grids that are not powers of two (wap_generic.cu)
 bool generic_size_supported(int n);

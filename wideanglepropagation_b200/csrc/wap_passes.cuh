@@ -176,28 +176,18 @@ struct RowCfg {
   static constexpr int PADN = RowExchange<true>::padded(NX);
 };
 
+// One row tile (rows blockDim.x / T consecutive rows of probe probe0 + by):
+// the body of row_pass_kernel and of the single-probe chain kernel.  tw is
+// the twiddle table in shared memory, xbuf the exchange buffer.
 template <int NX, int E>
-__global__ void __launch_bounds__(kRowThreads)
-row_pass_kernel(const RowArgs a) {
+__device__ __forceinline__ void row_pass_body(const RowArgs& a, const float4* tw, float2* xbuf, int bx, int by) {
   using C = RowCfg<NX, E>;
   constexpr int T = C::T;
   const int rows = blockDim.x / T;
-  extern __shared__ float4 smem_raw[];
-  float4* tw = smem_raw;
-  float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
-  // a plan's twiddles do not depend on the previous pass: their load overlaps
-  // its tail (one L2 round trip less on the chain of a single probe)
-  if (a.tw_ready)
-    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
-  pdl_wait_then_release();
-  if (!a.tw_ready)
-    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
-  __syncthreads();
-
   const int rl = threadIdx.x / T;
   const int t = threadIdx.x - rl * T;
-  const int row = blockIdx.x * rows + rl;
-  const int b = a.probe0 + blockIdx.y;
+  const int row = bx * rows + rl;
+  const int b = a.probe0 + by;
   const long long plane = (long long)a.ny * NX;
   float2* prow = a.psi + (long long)b * a.psi_bstride + (long long)row * NX;
   const RowExchange<C::WARP_LOCAL> xs{xbuf + rl * C::PADN};
@@ -307,6 +297,24 @@ row_pass_kernel(const RowArgs a) {
   for (int e = 0; e < E; ++e) __stcg(prow + t + T * e, v[e]);
 }
 
+template <int NX, int E>
+__global__ void __launch_bounds__(kRowThreads)
+row_pass_kernel(const RowArgs a) {
+  using C = RowCfg<NX, E>;
+  extern __shared__ float4 smem_raw[];
+  float4* tw = smem_raw;
+  float2* xbuf = reinterpret_cast<float2*>(tw + C::P::TW_SIZE);
+  // a plan's twiddles do not depend on the previous pass: their load overlaps
+  // its tail (one L2 round trip less on the chain of a single probe)
+  if (a.tw_ready)
+    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
+  pdl_wait_then_release();
+  if (!a.tw_ready)
+    for (int i = threadIdx.x; i < C::P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
+  __syncthreads();
+  row_pass_body<NX, E>(a, tw, xbuf, blockIdx.x, blockIdx.y);
+}
+
 // ----------------------------------------------------------------------------
 // column tiles: [NY][W] complex64 between global memory (row stride nx) and
 // shared memory, 16 bytes per access; consecutive threads take consecutive
@@ -337,29 +345,20 @@ __device__ __forceinline__ void tile_store(float2* __restrict__ g, const float2*
 // ----------------------------------------------------------------------------
 // column pass
 // ----------------------------------------------------------------------------
+// One column tile (W = blockDim.x / T columns of probe probe0 + by): the body
+// of col_pass_kernel and of the single-probe chain kernel.
 template <int NY, int E, bool SEED>
-__global__ void __launch_bounds__(kColThreads)
-col_pass_kernel(const ColArgs a) {
+__device__ __forceinline__ void col_pass_body(const ColArgs& a, const float4* tw, float2* tile, int bx, int by) {
   using P = FFTPlan<NY, E>;
   constexpr int T = P::T;
   const int W = blockDim.x / T;
-  extern __shared__ float4 smem_raw[];
-  float4* tw = smem_raw;
-  float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
-  if (a.tw_ready)
-    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
-  pdl_wait_then_release();
-  if (!a.tw_ready)
-    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
-  __syncthreads();
-
   const int c = threadIdx.x % W;
   const int t = threadIdx.x / W;
-  const int col = blockIdx.x * W + c;
-  const int b = a.probe0 + blockIdx.y;
+  const int col = bx * W + c;
+  const int b = a.probe0 + by;
   const int nx = a.nx;
   const long long plane = (long long)NY * nx;
-  float2* ptile = a.psi + (long long)b * a.psi_bstride + (long long)blockIdx.x * W;
+  float2* ptile = a.psi + (long long)b * a.psi_bstride + (long long)bx * W;
   const ColExchange<> xs{tile, W, c};
   const int f = a.flags;
 
@@ -400,7 +399,7 @@ col_pass_kernel(const ColArgs a) {
     if (a.seed2) {
       float2 u[E];
       __syncthreads();
-      tile_load<NY>(tile, a.seed2 + (long long)b * a.seed2_bstride + (long long)blockIdx.x * W, W, nx);
+      tile_load<NY>(tile, a.seed2 + (long long)b * a.seed2_bstride + (long long)bx * W, W, nx);
       __syncthreads();
 #pragma unroll
       for (int e = 0; e < E; ++e) u[e] = xs.ld(t + T * e);
@@ -462,6 +461,22 @@ col_pass_kernel(const ColArgs a) {
   for (int e = 0; e < E; ++e) xs.st(t + T * e, v[e]);
   __syncthreads();
   tile_store<NY>(ptile, tile, W, nx);
+}
+
+template <int NY, int E, bool SEED>
+__global__ void __launch_bounds__(kColThreads)
+col_pass_kernel(const ColArgs a) {
+  using P = FFTPlan<NY, E>;
+  extern __shared__ float4 smem_raw[];
+  float4* tw = smem_raw;
+  float2* tile = reinterpret_cast<float2*>(tw + P::TW_SIZE);
+  if (a.tw_ready)
+    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = __ldg(a.tw + i);
+  pdl_wait_then_release();
+  if (!a.tw_ready)
+    for (int i = threadIdx.x; i < P::TW_SIZE; i += blockDim.x) tw[i] = a.tw[i];
+  __syncthreads();
+  col_pass_body<NY, E, SEED>(a, tw, tile, blockIdx.x, blockIdx.y);
 }
 
 // The WPM bin propagator applied to v = X * Hvac by the direct formulas, for

@@ -388,6 +388,9 @@ def _prepare(potential, probe, positions, draw, dev):
 
 SCAN_SIZES = (128, 256, 512, 1024)
 SCAN_MIN_PROBES = 8
+# forwards of at most this many probes on these square grids run as one cooperative launch
+CHAIN_SIZES = (128, 256, 512, 1024, 2048)
+CHAIN_MAX_PROBES = 2
 _scans: dict = {}
 _scans_lock = threading.Lock()
 
@@ -549,8 +552,9 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     (``accumulate_patterns``), e.g. the frozen-phonon draws of each scan
     position into one float32 pattern per position; exit waves stay per probe.
 
-    Calls that run on the persistent scheduler (many probes of one probe)
-    raise WapError if one of its bounded device-side waits expired; with
+    Calls that run on the persistent scheduler (many probes of one probe) or
+    as one cooperative launch (one or two probes on a square 128-2048 grid)
+    raise WapError if one of their bounded device-side waits expired; with
     ``check=False`` the call returns without waiting for the GPU and the
     failure is raised by ``check_errors()`` or by a later call.
     """
@@ -581,6 +585,14 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), _ptr(H), _ptr(H_lo), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
         _ptr(stack), _stream()))
+    if B <= CHAIN_MAX_PROBES and ny == nx and ny in CHAIN_SIZES:
+        # one or two probes ran as one cooperative launch whose grid-wide waits are bounded
+        token = _lib.scan_status_begin(plan.handle, f"one-launch chain of {B} probe(s) on {ny}x{nx}, {N} slices",
+                                       source="wap_plan_status_async")
+        if check:
+            _lib.scan_status_end(token)
+        else:
+            _lib.defer_status(token)
     if accumulate is not None:
         dp = accumulate_patterns(dp, accumulate)
     if not batched:
