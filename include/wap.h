@@ -324,7 +324,7 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *   WAP_KNOB_ELEMS     elements per thread of forward scans: 16 or 8
  *   WAP_KNOB_TWIDDLES  stage-twiddle table: WAP_TW_FULL (hi + lo) or WAP_TW_HI
  *                      (hi only; by default scans of at most 160 slices)
- *   WAP_KNOB_TW_SMEM   1: twiddles in shared memory, 0: read through L1
+ *   WAP_KNOB_TW_SMEM   reserved (the twiddle image is always in shared memory)
  *   WAP_KNOB_PSI       how adjoint rows read psi_s: 0 global, 1 second stage,
  *                      2 the one stage refilled (default)
  *   WAP_KNOB_GROUP     probe-group size of classes that ask for automatic

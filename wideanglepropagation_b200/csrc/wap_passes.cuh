@@ -618,11 +618,8 @@ struct WpmColArgs {
   float dz;
 };
 
-// E = 8 instances are held to 64 registers, two 512-thread CTAs per SM (a
-// single probe's bins split over many CTAs needs the resident CTAs more than
-// it needs the spill-free register allocation)
 template <int NY, int E>
-__global__ void __launch_bounds__(kColThreads, E <= 8 ? 2 : 1)
+__global__ void __launch_bounds__(kColThreads)
 wpm_col_kernel(const WpmColArgs a) {
   using P = FFTPlan<NY, E>;
   constexpr int T = P::T;

@@ -181,12 +181,15 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// try_wait with a suspend-time hint: a waiting warp sleeps until the phase
+// completes (or the hint elapses) instead of re-issuing the test
+constexpr uint32_t kMbarSuspendNs = 1000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(phase)
+      : "r"(smem_u32(bar)), "r"(phase), "n"(kMbarSuspendNs)
       : "memory");
   return ok != 0;
 }
@@ -562,7 +565,9 @@ __device__ __forceinline__ void compute_loop_one(const SchedParams& P, float2* s
     const SchedClass& c = P.cls[k.cls];
     const Step st = step_of<GRAD>(c, k.pass);
     using TW = typename std::conditional<HI_TW, float2, float4>::type;
-    const TW* tw = P.tw_in_smem ? reinterpret_cast<const TW*>(tw_smem) + c.tw_off : reinterpret_cast<const TW*>(c.tw);
+    // always the shared-memory image: a pointer that could be either space
+    // would make every twiddle read a generic load
+    const TW* tw = reinterpret_cast<const TW*>(tw_smem) + c.tw_off;
     const bool col = step_is_col(st.type);
     // Adjoint rows read psi_s next to lambda.  kPsiStage2: both arrive
     // together (second stage), released after psi_s is read.  kPsiSplit:
@@ -668,7 +673,9 @@ __device__ __forceinline__ int tile_loop(const SchedParams& P, float2* stage, fl
     result = kLoopOther;
     const Step st = step_of<GRAD>(c, k.pass);
     using TW = typename std::conditional<HI_TW, float2, float4>::type;
-    const TW* tw = P.tw_in_smem ? reinterpret_cast<const TW*>(tw_smem) + c.tw_off : reinterpret_cast<const TW*>(c.tw);
+    // always the shared-memory image: a pointer that could be either space
+    // would make every twiddle read a generic load
+    const TW* tw = reinterpret_cast<const TW*>(tw_smem) + c.tw_off;
     const bool col = step_is_col(st.type);
     // Adjoint rows read psi_s next to lambda.  kPsiStage2: both arrive
     // together (second stage), released after psi_s is read.  kPsiSplit:
@@ -756,9 +763,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   __shared__ __align__(8) uint64_t full, empty, done_bar[2];
   __shared__ Task s_task;
 
-  if (P.tw_in_smem) {
-    for (int i = threadIdx.x; i < P.tw_image_len; i += blockDim.x) tw_smem[i] = P.tw_image[i];
-  }
+  for (int i = threadIdx.x; i < P.tw_image_len; i += blockDim.x) tw_smem[i] = P.tw_image[i];
   if (threadIdx.x == 0) {
     mbar_init(&full, 1);
     mbar_init(&empty, kComputeWarps);
@@ -1324,9 +1329,11 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   int per_sm_tw = 0;
   if ((rc0 = ctas_per_sm(s->kernel, base_smem, &per_sm)) || (rc0 = ctas_per_sm(s->kernel, base_smem + tw_smem_bytes, &per_sm_tw)))
     return rc0;
-  s->params.tw_in_smem = per_sm_tw >= per_sm && per_sm_tw > 0;
-  if (knob(WAP_KNOB_TW_SMEM) >= 0) s->params.tw_in_smem = knob(WAP_KNOB_TW_SMEM) != 0;
-  s->smem = base_smem + (s->params.tw_in_smem ? tw_smem_bytes : 0);
+  // the twiddle image always goes to shared memory (when it costs CTAs per
+  // SM, the launch simply has fewer)
+  s->params.tw_in_smem = 1;
+  (void)per_sm_tw;
+  s->smem = base_smem + tw_smem_bytes;
   if ((rc0 = ctas_per_sm(s->kernel, s->smem, &per_sm))) return rc0;
   if (per_sm < 1) return fail(WAP_ERR_CUDA, "scan_kernel does not fit on an SM");
   s->grid = sms * per_sm;

@@ -154,8 +154,9 @@ def solve_scattering_2d_lippmann_schwinger(potential_grid, energy_ev, pixel_size
     (volts, shape (Nx, Ny)) and a plane wave exp(i k0 y) along axis 1, by the
     Lippmann-Schwinger equation on a ``pad_factor``-padded grid
     (propagation.py:517-602).  ``absorb_frac`` / ``absorb_strength`` are
-    accepted and unused, as in the reference.  The padded grid times two must
-    be a power of two in [32, 2048] per axis.  Returns complex128 (Nx, Ny)."""
+    accepted and unused, as in the reference.  The padded grid times two (the
+    convolution grid) must be a power of two in [32, 2048] or any size in
+    [17, 1024] per axis (Bluestein transforms).  Returns complex128 (Nx, Ny)."""
     dev = _device()
     hbar = _HPLANCK / (2 * np.pi)
     gamma = 1.0 + energy_ev / (_ME * _C ** 2 / _QE)
