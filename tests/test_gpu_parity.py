@@ -237,9 +237,12 @@ def test_launch_configs_agree(wap):
 
 
 def test_unsupported_size_raises(wap):
-    with pytest.raises(ValueError, match="unsupported grid"):
-        wap.simulate_fresnel_as(np.zeros((1, 100, 100), np.float32), np.ones((100, 100), np.complex64),
-                                np.ones((100, 100), np.complex64), 1.0, 200e3)
+    """Sides beyond 1024 that are not powers of two (and below 17) are not
+    implemented; every other size is (the Bluestein path covers 17..1024)."""
+    for ny, nx in ((12, 64), (1500, 64)):
+        with pytest.raises(ValueError, match="unsupported grid"):
+            wap.simulate_fresnel_as(np.zeros((1, ny, nx), np.float32), np.ones((ny, nx), np.complex64),
+                                    np.ones((ny, nx), np.complex64), 1.0, 200e3)
 
 
 def test_pinned_host_inputs_upload_on_a_side_stream(wap):

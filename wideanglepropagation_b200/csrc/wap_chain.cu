@@ -152,9 +152,15 @@ static cudaError_t chain_launch_t(const ChainArgs& a, cudaStream_t st, int* grid
 static cudaError_t chain_launch(int n, int e, const ChainArgs& a, cudaStream_t st, int* grid) {
   switch (e * 100000 + n) {
     case 4 * 100000 + 128: return chain_launch_t<128, 4>(a, st, grid);
+    case 8 * 100000 + 128: return chain_launch_t<128, 8>(a, st, grid);
     case 4 * 100000 + 256: return chain_launch_t<256, 4>(a, st, grid);
+    case 8 * 100000 + 256: return chain_launch_t<256, 8>(a, st, grid);
+    case 16 * 100000 + 256: return chain_launch_t<256, 16>(a, st, grid);
+    case 4 * 100000 + 512: return chain_launch_t<512, 4>(a, st, grid);
     case 8 * 100000 + 512: return chain_launch_t<512, 8>(a, st, grid);
+    case 16 * 100000 + 512: return chain_launch_t<512, 16>(a, st, grid);
     case 8 * 100000 + 1024: return chain_launch_t<1024, 8>(a, st, grid);
+    case 16 * 100000 + 1024: return chain_launch_t<1024, 16>(a, st, grid);
     case 16 * 100000 + 2048: return chain_launch_t<2048, 16>(a, st, grid);
     default: return cudaErrorInvalidValue;
   }
@@ -162,13 +168,25 @@ static cudaError_t chain_launch(int n, int e, const ChainArgs& a, cudaStream_t s
 
 constexpr int kChainMaxProbes = 2;
 
+// The chain pays one grid-wide barrier per pass (about two microseconds) in
+// place of a launch; measured on B200 it wins where the per-pass chain is
+// bound by the host's launch rate (up to 256^2: C1 0.18 vs 0.23 ms per call)
+// and loses on larger grids (1024^2 x 100 slices: 3.58 vs 2.69 ms), so by
+// default it serves grids up to kChainMaxSize.  WAP_KNOB_CHAIN: 0 off, 1 the
+// default, 4 / 8 / 16 that many elements per thread on any chain size.
+constexpr int kChainMaxSize = 256;
+
 int chain_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes, int n_slices, float2* stack,
                   cudaStream_t st) {
   const int n = p->nx;
-  if (knob_value(WAP_KNOB_CHAIN) == 0) return -1;
+  const int kv = knob_value(WAP_KNOB_CHAIN);
+  if (kv == 0) return -1;
   if (p->generic || p->ny != n || n < 128 || n > 2048 || n_probes > kChainMaxProbes) return -1;
+  if (kv < 2 && n > kChainMaxSize) return -1;
   cudaError_t e;
-  const int E = chain_elems(n);
+  int E = chain_elems(n);
+  if (kv == 4 || kv == 8 || kv == 16) E = kv;
+  if (n / E > 128 || n / E < 8) return -1;   // whole rows and >= 2 column lanes per 256-thread CTA
   if (p->chain_e != E) {
     cudaFree(p->chain_tw);
     p->chain_tw = nullptr;

@@ -389,7 +389,7 @@ def _prepare(potential, probe, positions, draw, dev):
 SCAN_SIZES = (128, 256, 512, 1024)
 SCAN_MIN_PROBES = 8
 # forwards of at most this many probes on these square grids run as one cooperative launch
-CHAIN_SIZES = (128, 256, 512, 1024, 2048)
+CHAIN_SIZES = (128, 256)
 CHAIN_MAX_PROBES = 2
 _scans: dict = {}
 _scans_lock = threading.Lock()
@@ -553,7 +553,7 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     position into one float32 pattern per position; exit waves stay per probe.
 
     Calls that run on the persistent scheduler (many probes of one probe) or
-    as one cooperative launch (one or two probes on a square 128-2048 grid)
+    as one cooperative launch (one or two probes on a square 128 or 256 grid)
     raise WapError if one of their bounded device-side waits expired; with
     ``check=False`` the call returns without waiting for the GPU and the
     failure is raised by ``check_errors()`` or by a later call.
