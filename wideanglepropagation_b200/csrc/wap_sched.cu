@@ -117,6 +117,7 @@ struct SchedClass {
   const float2* ttab;           // (draws, N, n, n)  t / (n n)
   long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
+  const float2* Hh;             // (n, n) H_hi alone (the caller's complex64 H): hi-only instances
   float* dp;                    // (B, n, n) or null (a windowed class: the scan's full-grid scratch)
   // gradient buffers
   float2* lam;                  // (B, n, n) adjoint state
@@ -503,8 +504,22 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       }
     }
   }
-  const float4* hcol = c.Hq + col;
   const bool conj = GRAD && (type == ST_SEED_COL || type == ST_ADJ_COL);
+  if constexpr (std::is_same<TW, float2>::value) {
+    // hi-only instances (scans of at most kHiTwiddleMaxSlices slices): the
+    // propagator's hi part alone, like the stage twiddles - 8 bytes and four
+    // FMAs per element less; its rounding adds up over the slices as theirs
+    // does (4.5 -> 5.4e-6 exit-wave error on the 512^2 x 150-slice class)
+    const float2* hcol = c.Hh + col;
+    if (conj) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cmulc(v[e], __ldg(hcol + (t + T * e) * N));
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(hcol + (t + T * e) * N));
+    }
+  } else {
+  const float4* hcol = c.Hq + col;
   if (conj) {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -517,6 +532,7 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       const float4 h = __ldg(hcol + (t + T * e) * N);
       v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
     }
+  }
   }
   if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
@@ -1382,6 +1398,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
+    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc0 = bind_detector(s, c, ci))) return rc0;
     sc.vstride = (long long)c.n_slices * n * n;
@@ -1654,6 +1671,7 @@ int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
+    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc = bind_detector(s, c, ci))) return rc;
     s->cls[ci] = c;
