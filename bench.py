@@ -913,19 +913,29 @@ def _e2e(classes_host, args, dev, barrier, max_over_ranks, world, rank=0, max_an
             with torch.cuda.stream(down):
                 out.copy_(dp, non_blocking=True)
             dp.record_stream(down)
+        # steps are pipelined like a stream of scans: the next step's uploads
+        # and multislice overlap this step's last download (the downloads stay
+        # in order on their stream); finished runs' statuses are checked here
+        # without waiting, the rest after the loop
+        wap.propagation._lib.poll_errors()
+
+    def finish():
         torch.cuda.current_stream().wait_stream(down)
-        wap.check_errors()   # raises if a bounded device-side wait expired
 
     for _ in range(max(1, args.warmup)):
         step()
+    finish()
     torch.cuda.synchronize()
+    wap.check_errors()
     barrier()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
     for _ in range(args.steps):
         step()
+    finish()
     e.record()
     torch.cuda.synchronize()
+    wap.check_errors()   # raises if a bounded device-side wait expired in any timed step
     ms = max_over_ranks(s.elapsed_time(e)) / args.steps
     total = sum(w.n_probes * w.n_slices for w in classes_host)
     api = "simulate_fresnel_as(positions=, draw=, accumulate=per position)" if accumulate else \

@@ -312,10 +312,13 @@ int wap_scan_destroy(wap_scan* scan);
  * expire after `spin_limit` polls and the run reports WAP_ERR_TIMEOUT; pass
  * -1 restores normal operation.  No device fault is involved. */
 int wap_scan_debug_stall(wap_scan* scan, int pass, long long spin_limit);
-/* Debug validation (no counterpart in the reference): with on != 0 every
- * task is range-checked before use and a bad one is skipped; record (6 ints,
+/* Debug validation and counters (no counterpart in the reference): with
+ * on & 1 every task is range-checked before use and a bad one is skipped;
+ * with on & 2 the producers count the tickets whose inputs were not complete
+ * when claimed and the polls spent waiting for them.  record (8 ints,
  * nullable) receives [where, class, pass, probe, tile, valid] of the first
- * violation (where = 0: none). */
+ * violation (where = 0: none), then the two counters (cumulative since the
+ * scan was created; the second as an unsigned count). */
 int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
 /* Scheduler overrides for A/B timing and tests (no counterpart in the
  * reference), process-wide, read by every later wap_scan_create /

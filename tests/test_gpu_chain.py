@@ -49,16 +49,26 @@ def _per_pass(fn):
         _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_CHAIN, -1))
 
 
-@pytest.mark.parametrize("n,N", [(128, 9), (256, 20), (512, 12), (1024, 6), (2048, 3)])
-def test_chain_single_probe(wap, n, N):
+@pytest.mark.parametrize("n,N,elems", [(128, 9, 0), (256, 20, 0), (256, 8, 8), (512, 12, 4), (1024, 6, 8),
+                                       (2048, 3, 16)])
+def test_chain_single_probe(wap, n, N, elems):
+    """elems = 0: the default (128^2 and 256^2 run the chain); otherwise the
+    chain forced on with that many elements per thread (the A/B override,
+    which also reaches the larger grids)."""
     from oracle import propagation_oracle as O
     V, probe, ps, dz, E = _setup(n, N, seed=n)
     H = wap.angular_spectrum_propagation_kernel(n, n, (ps, ps), dz, E)
     call = lambda: wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=(n <= 512))
-    l0 = _lib.launch_count()
-    ex, dp, st = call()
-    torch.cuda.synchronize()
-    launches = _lib.launch_count() - l0
+    L = _lib.lib()
+    if elems:
+        _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_CHAIN, elems))
+    try:
+        l0 = _lib.launch_count()
+        ex, dp, st = call()
+        torch.cuda.synchronize()
+        launches = _lib.launch_count() - l0
+    finally:
+        _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_CHAIN, -1))
     assert launches <= 2, launches   # transmission table + the chain kernel
     pex, pdp, pst = _per_pass(call)
     rex, rdp, rst = O.simulate_fresnel_as(V.astype(np.float64), probe, H.cpu().numpy(), dz, E,

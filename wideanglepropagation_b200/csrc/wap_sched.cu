@@ -117,7 +117,6 @@ struct SchedClass {
   const float2* ttab;           // (draws, N, n, n)  t / (n n)
   long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
-  const float2* Hh;             // (n, n) H_hi alone (the caller's complex64 H): hi-only instances
   float* dp;                    // (B, n, n) or null (a windowed class: the scan's full-grid scratch)
   // gradient buffers
   float2* lam;                  // (B, n, n) adjoint state
@@ -258,7 +257,7 @@ __device__ __forceinline__ Step step_of(const SchedClass& c, int pass) {
 // and report whether the task may be used.
 template <bool GRAD>
 __device__ __forceinline__ bool task_ok(const SchedParams& P, const Task& k, int where) {
-  if (!P.checks) return true;
+  if (!(P.checks & 1)) return true;
   bool ok = k.cls >= 0 && k.cls < P.n_classes;
   if (ok) {
     const SchedClass& c = P.cls[k.cls];
@@ -504,22 +503,8 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       }
     }
   }
-  const bool conj = GRAD && (type == ST_SEED_COL || type == ST_ADJ_COL);
-  if constexpr (std::is_same<TW, float2>::value) {
-    // hi-only instances (scans of at most kHiTwiddleMaxSlices slices): the
-    // propagator's hi part alone, like the stage twiddles - 8 bytes and four
-    // FMAs per element less; its rounding adds up over the slices as theirs
-    // does (4.5 -> 5.4e-6 exit-wave error on the 512^2 x 150-slice class)
-    const float2* hcol = c.Hh + col;
-    if (conj) {
-#pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = cmulc(v[e], __ldg(hcol + (t + T * e) * N));
-    } else {
-#pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(hcol + (t + T * e) * N));
-    }
-  } else {
   const float4* hcol = c.Hq + col;
+  const bool conj = GRAD && (type == ST_SEED_COL || type == ST_ADJ_COL);
   if (conj) {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -532,7 +517,6 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       const float4 h = __ldg(hcol + (t + T * e) * N);
       v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
     }
-  }
   }
   if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
@@ -838,6 +822,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
       __nanosleep(ns);
       if (ns < 1024) ns <<= 1;
     }
+    if ((P.checks & 2) && spins) atomicAdd(reinterpret_cast<unsigned*>(P.debug) + 7, (unsigned)spins);
     fence_proxy_async();
     return true;
   };
@@ -879,7 +864,9 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   while (k.valid) {
     Task kn = claim();
     bool issued = false;
-    if (kn.valid && ld_acquire(counter_of(kn)) >= need_of(kn)) {
+    const bool ready = kn.valid && ld_acquire(counter_of(kn)) >= need_of(kn);
+    if ((P.checks & 2) && kn.valid && !ready) atomicAdd(P.debug + 6, 1);
+    if (ready) {
       // inputs ready: stream the next tile in as soon as the stage is free
       if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
       eph ^= 1u;
@@ -1398,7 +1385,6 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
-    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc0 = bind_detector(s, c, ci))) return rc0;
     sc.vstride = (long long)c.n_slices * n * n;
@@ -1671,7 +1657,6 @@ int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
-    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc = bind_detector(s, c, ci))) return rc;
     s->cls[ci] = c;
@@ -1795,7 +1780,7 @@ int wap_scan_debug_checks(wap_scan* s, int on, int* record) {
   if (!s) return fail(WAP_ERR_ARG, "scan is NULL");
   s->params.checks = on;
   if (record) {
-    cudaError_t e = cudaMemcpy(record, s->d_debug, 6 * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(record, s->d_debug, 8 * sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "scan debug record");
   }
   return WAP_OK;
