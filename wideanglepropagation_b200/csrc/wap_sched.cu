@@ -858,21 +858,36 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   };
 
   uint32_t tiles_signalled = 0;
+  auto ready_now = [&](const Task& t) -> bool {
+    const bool r = t.valid && ld_acquire(counter_of(t)) >= need_of(t);
+    if ((P.checks & 2) && t.valid && !r) atomicAdd(P.debug + 6, 1);
+    return r;
+  };
+  Task none;
+  none.valid = 0;
+  none.cls = none.pass = none.b = none.tile = 0;
   Task k = claim();
   if (k.valid && !wait_ready(k)) k.valid = 0;
   publish(k);
+  // The ticket after the one being computed is claimed and checked while that
+  // one computes (the claim's atomic and the readiness load are round trips
+  // to L2), so that it can be published the moment the stage frees.
+  Task kn = k.valid ? claim() : none;
+  bool rn = ready_now(kn);
   while (k.valid) {
-    Task kn = claim();
     bool issued = false;
-    const bool ready = kn.valid && ld_acquire(counter_of(kn)) >= need_of(kn);
-    if ((P.checks & 2) && kn.valid && !ready) atomicAdd(P.debug + 6, 1);
-    if (ready) {
-      // inputs ready: stream the next tile in as soon as the stage is free
+    Task kn2 = none;
+    bool rn2 = false;
+    if (rn) {
+      // inputs ready: stream kn in as soon as the stage is free, then claim
+      // the ticket after it
       if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
       eph ^= 1u;
       fence_proxy_async();
       publish(kn);
       issued = true;
+      kn2 = claim();
+      rn2 = ready_now(kn2);
     }
     // completion of k: every compute warp has stored its part.  The compute
     // warps may already have finished the prefetched tile too, so tiles
@@ -891,8 +906,14 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
       if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
       eph ^= 1u;
       publish(kn);   // kn or the stop sentinel
+      if (kn.valid) {
+        kn2 = claim();
+        rn2 = ready_now(kn2);
+      }
     }
     k = kn;
+    kn = kn2;
+    rn = rn2;
   }
   // After an error the compute warps may have stopped without consuming the
   // last published tile: let its copy land (bounded) before the CTA exits.
