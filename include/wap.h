@@ -332,14 +332,17 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *                      2 the one stage refilled (default)
  *   WAP_KNOB_GROUP     probe-group size of classes that ask for automatic
  *   WAP_KNOB_CHAIN     0: single-probe forwards as one launch per pass instead
- *                      of the one-launch chain kernel (default 1) */
+ *                      of the one-launch chain kernel (default 1)
+ *   WAP_KNOB_SUSPEND   suspend-time hint (ns) of the scheduler's mbarrier
+ *                      waits, 0: none (default 1000) */
 #define WAP_KNOB_ELEMS 0
 #define WAP_KNOB_TWIDDLES 1
 #define WAP_KNOB_TW_SMEM 2
 #define WAP_KNOB_PSI 3
 #define WAP_KNOB_GROUP 4
 #define WAP_KNOB_CHAIN 5
-#define WAP_KNOB_COUNT 6
+#define WAP_KNOB_SUSPEND 6
+#define WAP_KNOB_COUNT 7
 #define WAP_TW_FULL 1
 #define WAP_TW_HI 2
 int wap_scan_debug_override(int which, int value);

@@ -164,6 +164,7 @@ struct alignas(64) SchedParams {
   int tw_image_len;                // its entries
   int stage2;                      // how adjoint rows get psi_s: kPsiGlobal / kPsiStage2 / kPsiSplit
   int* debug;                      // [code, cls, step, b, tile, extra] of the first bad task
+  unsigned suspend_ns;             // mbarrier wait suspend-time hint (0: none)
 };
 
 // ---------------------------------------------------------------------------
@@ -181,22 +182,30 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// try_wait with a suspend-time hint: a waiting warp sleeps until the phase
-// completes (or the hint elapses) instead of re-issuing the test
+// try_wait with a suspend-time hint (ns; 0: none): a waiting warp may sleep
+// until the phase completes or the hint elapses instead of re-issuing the test
 constexpr uint32_t kMbarSuspendNs = 1000;
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase, uint32_t hint_ns) {
   uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(phase), "n"(kMbarSuspendNs)
-      : "memory");
+  if (hint_ns) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(hint_ns)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+  }
   return ok != 0;
 }
 // bounded mbarrier wait; false if the limit expired
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit, uint32_t hint_ns) {
   long long spins = 0;
-  while (!mbar_try_wait(bar, phase)) {
+  while (!mbar_try_wait(bar, phase, hint_ns)) {
     if (++spins > limit) return false;
   }
   return true;
@@ -548,7 +557,7 @@ __device__ __forceinline__ void compute_loop_one(const SchedParams& P, float2* s
     // and keep waiting (bounded rounds): the producer's own waits are bounded
     // and it publishes the stop sentinel once an error is recorded, so every
     // compute warp reads the same item and runs the same barrier sequence.
-    for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit); ++round)
+    for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit, P.suspend_ns); ++round)
       atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
     fph ^= 1u;
     const Task k = *s_task;
@@ -580,7 +589,7 @@ __device__ __forceinline__ void compute_loop_one(const SchedParams& P, float2* s
     const float2* st2 = late ? stage + kTileBytesFor(E) / sizeof(float2) : split ? stage : nullptr;
     auto acquire = [&]() {
       if (split) {
-        for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit); ++round)
+        for (int round = 0; round < 4 && !mbar_wait(full, fph, P.spin_limit, P.suspend_ns); ++round)
           atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
         fph ^= 1u;
       }
@@ -647,7 +656,7 @@ __device__ __forceinline__ int tile_loop(const SchedParams& P, float2* stage, fl
       // and keep waiting (bounded rounds): the producer's own waits are bounded
       // and it publishes the stop sentinel once an error is recorded, so every
       // compute warp reads the same item and runs the same barrier sequence.
-      for (int round = 0; round < 4 && !mbar_wait(full, cs.fph, P.spin_limit); ++round)
+      for (int round = 0; round < 4 && !mbar_wait(full, cs.fph, P.spin_limit, P.suspend_ns); ++round)
         atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
       cs.fph ^= 1u;
       cs.k = *s_task;
@@ -688,7 +697,7 @@ __device__ __forceinline__ int tile_loop(const SchedParams& P, float2* stage, fl
     const float2* st2 = late ? stage + kTileBytesFor(E) / sizeof(float2) : split ? stage : nullptr;
     auto acquire = [&]() {
       if (split) {
-        for (int round = 0; round < 4 && !mbar_wait(full, cs.fph, P.spin_limit); ++round)
+        for (int round = 0; round < 4 && !mbar_wait(full, cs.fph, P.spin_limit, P.suspend_ns); ++round)
           atomicCAS(P.status, 0, WAP_ERR_TIMEOUT);
         cs.fph ^= 1u;
       }
@@ -847,7 +856,7 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
     if (GRAD && P.stage2 == kPsiSplit && (type == ST_ADJ_ROW || type == ST_ADJ_ROW0)) {
       // second phase of the same tile: once every compute warp holds lambda,
       // refill the stage with the matching rows of psi_s
-      if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
+      if (!mbar_wait(&empty, eph, P.spin_limit, P.suspend_ns)) fail_wait();
       eph ^= 1u;
       fence_proxy_async();
       const Step st = step_of<GRAD>(c, k.pass);
@@ -858,43 +867,31 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
   };
 
   uint32_t tiles_signalled = 0;
-  auto ready_now = [&](const Task& t) -> bool {
-    const bool r = t.valid && ld_acquire(counter_of(t)) >= need_of(t);
-    if ((P.checks & 2) && t.valid && !r) atomicAdd(P.debug + 6, 1);
-    return r;
-  };
-  Task none;
-  none.valid = 0;
-  none.cls = none.pass = none.b = none.tile = 0;
   Task k = claim();
   if (k.valid && !wait_ready(k)) k.valid = 0;
   publish(k);
-  // The ticket after the one being computed is claimed and checked while that
-  // one computes (the claim's atomic and the readiness load are round trips
-  // to L2), so that it can be published the moment the stage frees.
-  Task kn = k.valid ? claim() : none;
-  bool rn = ready_now(kn);
   while (k.valid) {
+    // the next ticket is claimed only now: claiming it while k still computes
+    // (one tile earlier) found its inputs incomplete for a third of the tickets
+    // of the headline scan and cost 4 % (56.8 against 54.5 ms)
+    Task kn = claim();
     bool issued = false;
-    Task kn2 = none;
-    bool rn2 = false;
-    if (rn) {
-      // inputs ready: stream kn in as soon as the stage is free, then claim
-      // the ticket after it
-      if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
+    const bool ready = kn.valid && ld_acquire(counter_of(kn)) >= need_of(kn);
+    if ((P.checks & 2) && kn.valid && !ready) atomicAdd(P.debug + 6, 1);
+    if (ready) {
+      // inputs ready: stream the next tile in as soon as the stage is free
+      if (!mbar_wait(&empty, eph, P.spin_limit, P.suspend_ns)) fail_wait();
       eph ^= 1u;
       fence_proxy_async();
       publish(kn);
       issued = true;
-      kn2 = claim();
-      rn2 = ready_now(kn2);
     }
     // completion of k: every compute warp has stored its part.  The compute
     // warps may already have finished the prefetched tile too, so tiles
     // alternate between two barriers (a parity wait never sees two phases).
     {
       const int q = tiles_signalled & 1;
-      if (!mbar_wait(&done_bar[q], dph[q], P.spin_limit)) fail_wait();
+      if (!mbar_wait(&done_bar[q], dph[q], P.spin_limit, P.suspend_ns)) fail_wait();
       dph[q] ^= 1u;
       ++tiles_signalled;
     }
@@ -903,21 +900,15 @@ __global__ void __launch_bounds__(kBlockThreads, E == 16 ? 3 : 4) scan_kernel(co
     if (!issued) {
       // holding nothing unsignalled now: safe to block on kn's inputs
       if (kn.valid && !wait_ready(kn)) kn.valid = 0;
-      if (!mbar_wait(&empty, eph, P.spin_limit)) fail_wait();
+      if (!mbar_wait(&empty, eph, P.spin_limit, P.suspend_ns)) fail_wait();
       eph ^= 1u;
       publish(kn);   // kn or the stop sentinel
-      if (kn.valid) {
-        kn2 = claim();
-        rn2 = ready_now(kn2);
-      }
     }
     k = kn;
-    kn = kn2;
-    rn = rn2;
   }
   // After an error the compute warps may have stopped without consuming the
   // last published tile: let its copy land (bounded) before the CTA exits.
-  if (load_out && *(volatile int*)P.status != 0) mbar_wait(&full, fph ^ 1u, P.spin_limit);
+  if (load_out && *(volatile int*)P.status != 0) mbar_wait(&full, fph ^ 1u, P.spin_limit, P.suspend_ns);
 }
 
 // dL/dV += 2 dphi/dV(V) S for every voxel, S being the probes' sum of
@@ -1090,7 +1081,7 @@ static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n 
 // Scheduler overrides for A/B timing and tests (wap_scan_debug_override); -1:
 // the library's own choice.  Set only by an explicit call, never from the
 // environment, and read when a scan is created.
-static int g_knob[WAP_KNOB_COUNT] = {-1, -1, -1, -1, -1, -1};
+static int g_knob[WAP_KNOB_COUNT] = {-1, -1, -1, -1, -1, -1, -1};
 static int knob(int k) { return g_knob[k]; }
 namespace wap {
 int knob_value(int k) { return (k >= 0 && k < WAP_KNOB_COUNT) ? g_knob[k] : -1; }
@@ -1518,6 +1509,7 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
   s->params.done = s->d_done;
   s->params.status = s->d_status;
   s->params.spin_limit = kSpinLimit;
+  s->params.suspend_ns = knob(WAP_KNOB_SUSPEND) >= 0 ? (unsigned)knob(WAP_KNOB_SUSPEND) : kMbarSuspendNs;
   s->params.stall_pass = -1;
   s->params.checks = 0;
   s->params.debug = s->d_debug;
