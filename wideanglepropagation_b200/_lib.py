@@ -25,7 +25,7 @@ WAP_TF_FRESNEL = 0
 WAP_TF_ANGULAR = 1
 
 (WAP_KNOB_ELEMS, WAP_KNOB_TWIDDLES, WAP_KNOB_TW_SMEM, WAP_KNOB_PSI, WAP_KNOB_GROUP, WAP_KNOB_CHAIN,
- WAP_KNOB_SUSPEND) = range(7)
+ WAP_KNOB_SUSPEND, WAP_KNOB_H_HI) = range(8)
 WAP_TW_FULL = 1
 WAP_TW_HI = 2
 
