@@ -334,10 +334,8 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *   WAP_KNOB_CHAIN     0: single-probe forwards as one launch per pass instead
  *                      of the one-launch chain kernel (default 1)
  *   WAP_KNOB_SUSPEND   suspend-time hint (ns) of the scheduler's mbarrier
- *                      waits, 0: none (default 1000)
- *   WAP_KNOB_H_HI      1: every class of a hi-only scan applies the propagator's
- *                      hi part alone, 0: none (default: classes of at most
- *                      100 slices) */
+ *                      waits, 0: none (the default)
+ *   WAP_KNOB_H_HI      reserved */
 #define WAP_KNOB_ELEMS 0
 #define WAP_KNOB_TWIDDLES 1
 #define WAP_KNOB_TW_SMEM 2

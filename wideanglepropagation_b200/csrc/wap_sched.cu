@@ -117,8 +117,6 @@ struct SchedClass {
   const float2* ttab;           // (draws, N, n, n)  t / (n n)
   long long vstride;            // N n n (draw stride of V, ttab, grad)
   const float4* Hq;             // (n, n) interleaved (H_hi, H_lo)
-  const float2* Hh;             // (n, n) H_hi alone (the caller's complex64 H)
-  int h_hi;                     // apply H_hi alone (hi-only instances, short classes)
   float* dp;                    // (B, n, n) or null (a windowed class: the scan's full-grid scratch)
   // gradient buffers
   float2* lam;                  // (B, n, n) adjoint state
@@ -186,7 +184,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 // try_wait with a suspend-time hint (ns; 0: none): a waiting warp may sleep
 // until the phase completes or the hint elapses instead of re-issuing the test
-constexpr uint32_t kMbarSuspendNs = 1000;
+// (measured on the headline scan: 0, 200, 1000 and 4000 ns within 0.2 %)
+constexpr uint32_t kMbarSuspendNs = 0;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase, uint32_t hint_ns) {
   uint32_t ok;
   if (hint_ns) {
@@ -339,11 +338,6 @@ constexpr int kComputeWarps = kSchedThreads / 32;      // 8 compute warps
 constexpr int kBlockThreads = kSchedThreads + 32;       // + 1 producer warp
 // forward scans of at most this many slices use hi-only stage twiddles
 constexpr int kHiTwiddleMaxSlices = 160;
-// classes of at most this many slices (in hi-only instances) apply the
-// propagator's hi part alone: measured on the headline scan, the 256^2 x 80
-// class moves from 2.2e-6 / 3.1e-6 to 2.8e-6 / 4.2e-6 (exit / pattern error
-// against float64), below the 512^2 x 150 class's 4.5e-6 / 7.3e-6 with hi + lo
-constexpr int kHiHMaxSlices = 100;
 constexpr int kFftBar = 2;                              // named barrier of the compute warps
 
 // ---------------------------------------------------------------------------
@@ -520,19 +514,6 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
     }
   }
   const bool conj = GRAD && (type == ST_SEED_COL || type == ST_ADJ_COL);
-  if (std::is_same<TW, float2>::value && c.h_hi) {
-    // the propagator's hi part alone (8 B and four FMAs per element less):
-    // only for classes short enough that its rounding, applied identically
-    // at every slice, stays below the error of the longest class
-    const float2* hh = c.Hh + col;
-    if (conj) {
-#pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = cmulc(v[e], __ldg(hh + (t + T * e) * N));
-    } else {
-#pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = cmul(v[e], __ldg(hh + (t + T * e) * N));
-    }
-  } else {
   const float4* hcol = c.Hq + col;
   if (conj) {
 #pragma unroll
@@ -546,7 +527,6 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
       const float4 h = __ldg(hcol + (t + T * e) * N);
       v[e] = cmul_hl(v[e], make_float2(h.x, h.y), make_float2(h.z, h.w));
     }
-  }
   }
   if (!GRAD && c.dp && st.slice == c.n_slices - 1) {
     float* dp = c.dp + (long long)k.b * plane;
@@ -1161,8 +1141,10 @@ static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map
 
 // Trailing checkpoint segments whose waves the forward keeps, so that the
 // backward recomputes none of them: memory stays O(sqrt N) - checkpoints every
-// k slices plus 2k waves - and one segment's recompute (2k - 1 passes) drops.
-constexpr int kKeptSegments = 2;
+// k slices plus 3k waves - and three segments' recompute (2k - 1 passes each)
+// drop.  Two kept segments left the 512^2 x 64-slice gradient step at 3.03 x
+// its forward after the forward scan itself had become faster.
+constexpr int kKeptSegments = 3;
 
 static int kept_first_slice(int n_slices, int k) {
   const int nck = (n_slices + k - 1) / k;
@@ -1348,13 +1330,6 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     }
   }
   const int tw_total = (int)image.size();
-  // classes whose propagator is applied as its hi part alone: hi-only
-  // instances, classes of at most kHiHMaxSlices slices
-  for (int ci = 0; ci < n_classes; ++ci) {
-    const int kv = knob(WAP_KNOB_H_HI);
-    s->params.cls[ci].h_hi =
-        s->hi_tw && (kv == 1 || (kv < 0 && classes[ci].n_slices <= kHiHMaxSlices)) ? 1 : 0;
-  }
   s->kernel = s->hi_tw ? pick_fwd_hi(mask) : E == 8 ? pick_fwd_e<8>(mask) : pick_fwd_e<16>(mask);
   if (s->grad) s->kernel_bwd = s->hi_tw ? pick_grad<true>(mask) : pick_grad<false>(mask);
   // Keep the twiddles in shared memory only when they fit next to the stage
@@ -1425,7 +1400,6 @@ static int scan_setup(wap_scan* s, int n_classes, const wap_scan_class* classes,
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
-    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc0 = bind_detector(s, c, ci))) return rc0;
     sc.vstride = (long long)c.n_slices * n * n;
@@ -1699,7 +1673,6 @@ int wap_scan_bind(wap_scan* s, int n_classes, const wap_scan_class* classes) {
     sc.positions = c.positions;
     sc.draw = c.draw;
     sc.V = c.V;
-    sc.Hh = reinterpret_cast<const float2*>(c.H);
     sc.dp = c.dp;
     if ((rc = bind_detector(s, c, ci))) return rc;
     s->cls[ci] = c;
