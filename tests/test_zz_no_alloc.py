@@ -3,10 +3,11 @@ device memory while they run (graph capture under a framework that forbids
 allocation, fixed-pool hosts, plugin hosts that only hand over buffers).
 
 Collected last on purpose.  Calls the entry point through the C ABI twice in
-a row (the second call reuses the library's fixed scratch array) and checks
-both results against wap_multislice_fwd (the regular entry point) within the
-parity tolerance of the other GPU tests.  Runs alone in a fresh process or
-after the rest of the suite.
+a row (the second call reuses the library's fixed scratch array and takes no
+device memory) and records it into a CUDA graph, checking every result against
+wap_multislice_fwd (the regular entry point) within the parity tolerance of
+the other GPU tests.  Runs alone in a fresh process or after the rest of the
+suite.
 """
 import ctypes
 
@@ -69,6 +70,68 @@ def test_noalloc_matches_regular_entry_point(ny, nx, B):
         assert rel(ex, ref_exit) < TOL, call
         assert rel(dp, ref_dp) < TOL, call
         assert rel(st, ref_stack) < TOL, call
+
+
+def test_noalloc_captures_in_cuda_graph():
+    """The documented use: the call recorded into a CUDA graph in global
+    capture mode (which fails any allocation or synchronising call made while
+    capturing), then replayed twice with new inputs copied into the captured
+    buffers; each replay matches the regular entry point."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from wideanglepropagation_b200 import _lib
+    from wideanglepropagation_b200.propagation import get_plan, split_transfer
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ny = nx = 256
+    B, N, dz, E = 2, 4, 2.0, 200e3
+    rng = np.random.default_rng(7)
+    p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
+    H128 = torch.exp(1j * torch.as_tensor(rng.uniform(-3, 3, (ny, nx)), device=dev))
+    H, H_lo = split_transfer(H128, dev)
+    pos = torch.as_tensor(np.array([[5, 200], [128, 17]], np.int32), device=dev)
+    V = torch.empty((N, ny, nx), dtype=torch.float32, device=dev)
+    probe = torch.empty((ny, nx), dtype=torch.complex64, device=dev)
+    ex = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
+    dp = torch.empty((B, ny, nx), dtype=torch.float32, device=dev)
+
+    def inputs(seed):
+        r = np.random.default_rng(seed)
+        V.copy_(torch.as_tensor(r.uniform(0, 40, (N, ny, nx)).astype(np.float32)))
+        probe.copy_(torch.as_tensor((r.normal(size=(ny, nx)) + 1j * r.normal(size=(ny, nx))).astype(np.complex64)))
+
+    def reference():
+        plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
+        rex = torch.empty_like(ex)
+        rdp = torch.empty_like(dp)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.wap_multislice_fwd(plan.handle, p(V), N, 1, None, p(probe), B, 0, p(pos), p(H), p(H_lo), dz, E,
+                                        p(rex), p(dp), None, st))
+        torch.cuda.synchronize()
+        return rex, dp.clone()
+
+    side = torch.cuda.Stream()
+    inputs(1)
+    with torch.cuda.stream(side):   # warm-up outside the capture (first use loads the kernels)
+        _lib.check(L.wap_multislice_fwd_noalloc(p(V), N, ny, nx, p(probe), B, 0, p(pos), p(H), p(H_lo), dz, E,
+                                                p(ex), p(dp), None, ctypes.c_void_p(side.cuda_stream)))
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side, capture_error_mode="global"):
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.wap_multislice_fwd_noalloc(p(V), N, ny, nx, p(probe), B, 0, p(pos), p(H), p(H_lo), dz, E,
+                                                p(ex), p(dp), None, st))
+    for seed in (2, 3):
+        inputs(seed)
+        rex, rdp = reference()
+        ex.fill_(float("nan"))
+        dp.fill_(float("nan"))
+        g.replay()
+        torch.cuda.synchronize()
+        assert rel(ex, rex) < TOL, seed
+        assert rel(dp, rdp) < TOL, seed
+    del g
 
 
 def test_noalloc_rejects_bad_sizes():
