@@ -60,6 +60,11 @@ int wap_plan_destroy(wap_plan* plan);
  * memory, enqueued on `stream`; valid once the stream reaches it.  No
  * counterpart in the reference. */
 int wap_plan_status_async(wap_plan* plan, int* host_status, void* stream);
+/* *pending = 1 when the last wap_multislice_fwd on this plan ran the one-launch
+ * chain (so wap_plan_status_async has a status to report), else 0 (the
+ * cluster kernel and the per-pass launches have no device-side waits).  Host
+ * only.  No counterpart in the reference. */
+int wap_plan_status_pending(wap_plan* plan, int* pending);
 
 /* FFT launch shape of the row pass (elements per thread) and column pass
  * (elements per thread, columns per CTA); set by the autotuner.  Elements
@@ -335,7 +340,10 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *                      of the one-launch chain kernel (default 1)
  *   WAP_KNOB_SUSPEND   suspend-time hint (ns) of the scheduler's mbarrier
  *                      waits, 0: none (the default)
- *   WAP_KNOB_H_HI      reserved */
+ *   WAP_KNOB_H_HI      reserved
+ *   WAP_KNOB_CLUSTER   0: single-probe forwards without the cluster kernel
+ *                      (wave in distributed shared memory); 4 / 8 / 16 that
+ *                      many elements per thread */
 #define WAP_KNOB_ELEMS 0
 #define WAP_KNOB_TWIDDLES 1
 #define WAP_KNOB_TW_SMEM 2
@@ -344,7 +352,8 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
 #define WAP_KNOB_CHAIN 5
 #define WAP_KNOB_SUSPEND 6
 #define WAP_KNOB_H_HI 7
-#define WAP_KNOB_COUNT 8
+#define WAP_KNOB_CLUSTER 8
+#define WAP_KNOB_COUNT 9
 #define WAP_TW_FULL 1
 #define WAP_TW_HI 2
 int wap_scan_debug_override(int which, int value);

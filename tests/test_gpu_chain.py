@@ -1,7 +1,9 @@
 """One-launch chain of a single probe (cooperative kernel, grid-wide barriers
 between the passes): against the FP64 oracle and against the per-pass path
 (one launch per pass, forced through wap_scan_debug_override), on every chain
-size, with two probes, the wavefront stack and a detector window.
+size, with two probes, the wavefront stack and a detector window.  The
+cluster kernel, which serves 128^2 and 256^2 by default, is switched off for
+these tests.
 
 Tolerance: rel-L2 <= 1e-5 against the oracle; the chain and the per-pass
 launches may use different elements per thread (FFT radix plans), so they
@@ -23,7 +25,12 @@ def wap():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     import wideanglepropagation_b200 as w
-    return w
+    # 128^2 / 256^2 probes take the cluster kernel by default: off here, so
+    # that these sizes reach the chain
+    L = _lib.lib()
+    _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_CLUSTER, 0))
+    yield w
+    _lib.check(L.wap_scan_debug_override(_lib.WAP_KNOB_CLUSTER, -1))
 
 
 def rel(a, b):

@@ -25,7 +25,7 @@ WAP_TF_FRESNEL = 0
 WAP_TF_ANGULAR = 1
 
 (WAP_KNOB_ELEMS, WAP_KNOB_TWIDDLES, WAP_KNOB_TW_SMEM, WAP_KNOB_PSI, WAP_KNOB_GROUP, WAP_KNOB_CHAIN,
- WAP_KNOB_SUSPEND, WAP_KNOB_H_HI) = range(8)
+ WAP_KNOB_SUSPEND, WAP_KNOB_H_HI, WAP_KNOB_CLUSTER) = range(9)
 WAP_TW_FULL = 1
 WAP_TW_HI = 2
 
@@ -66,6 +66,7 @@ SIGNATURES = {
     "wap_scan_status": (_I, [_P, ctypes.POINTER(_I)]),
     "wap_scan_status_async": (_I, [_P, _P, _P]),
     "wap_plan_status_async": (_I, [_P, _P, _P]),
+    "wap_plan_status_pending": (_I, [_P, ctypes.POINTER(_I)]),
     "wap_scan_debug_override": (_I, [_I, _I]),
     "wap_scan_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "wap_scan_destroy": (_I, [_P]),
@@ -135,27 +136,55 @@ _pending: list = []
 _pending_lock = threading.Lock()
 
 
-def scan_status_begin(handle, what: str, source: str = "wap_scan_status_async"):
-    """Enqueue, on the current stream, a copy of a scan's (or, with
-    source="wap_plan_status_async", a plan's one-launch chain's) status word
-    into pinned host memory and record an event after it; returns the token
-    that ``scan_status_end`` or ``defer_status`` take."""
+# Reusable (event, pinned status word, numpy view of it) triples per device:
+# a token takes one and gives it back once its status has been read, so a call
+# pays neither a pinned allocation nor an event creation.
+_token_pool: dict = {}
+
+
+def _token_parts(device_index: int):
+    with _pending_lock:
+        pool = _token_pool.get(device_index)
+        if pool:
+            return pool.pop()
     import torch
     word = torch.zeros(1, dtype=torch.int32, pin_memory=True)
-    stream = torch.cuda.current_stream()
+    return torch.cuda.Event(), word, word.numpy()
+
+
+def scan_status_begin(handle, what: str, source: str = "wap_scan_status_async", stream=None):
+    """Enqueue, on ``stream`` (default: the current one), a copy of a scan's
+    (or, with source="wap_plan_status_async", a plan's one-launch chain's)
+    status word into pinned host memory and record an event after it; returns
+    the token that ``scan_status_end`` or ``defer_status`` take."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    di = stream.device.index
+    ev, word, view = _token_parts(di)
+    view[0] = 0
     check(getattr(lib(), source)(handle, ctypes.c_void_p(word.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
-    ev = torch.cuda.Event()
     ev.record(stream)
-    return ev, word, what
+    return ev, word, what, view, di
 
 
 def _raise_status(token) -> None:
-    ev, word, what = token
+    ev, word, what, view, di = token
     ev.synchronize()
-    st = int(word[0])
+    st = int(view[0])
+    with _pending_lock:
+        _token_pool.setdefault(di, []).append((ev, word, view))
     if st != WAP_OK:
         kind = "a bounded device-side wait expired" if st == WAP_ERR_TIMEOUT else "the kernel reported an error"
         raise WapError(f"libwap error {st}: {what}: {kind}; its outputs are incomplete")
+
+
+def plan_status_pending(handle) -> bool:
+    """Whether the last forward on the plan ran the one-launch chain (the only
+    single-probe path with device-side waits, so the only one with a status)."""
+    v = ctypes.c_int(0)
+    check(lib().wap_plan_status_pending(handle, ctypes.byref(v)))
+    return bool(v.value)
 
 
 def scan_status_end(token) -> None:

@@ -350,6 +350,7 @@ static void plan_free(wap_plan* p) {
   cudaFree(p->chain_tw);
   cudaFree(p->chain_count);
   cudaFree(p->chain_status);
+  cudaFree(p->cl_tw);
   if (p->generic) {
     generic_axis_free(&p->gen_x);
     generic_axis_free(&p->gen_y);
@@ -634,8 +635,16 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   r.src = reinterpret_cast<const float2*>(psi0);
   r.src_bstride = psi0_per_probe ? plane : 0;
   r.shifts = positions;
+  ColArgs c = base_col_args(p, H, H_lo);
+  c.psi = r.psi;
+  c.psi_bstride = plane;
+  c.dp = dp;
+  p->chain_ran = 0;
   // exp(i phi(V)) tabulated once per (draw, slice) (use_trans_table), else
-  // evaluated inline by the row pass
+  // evaluated inline by the row pass.  (The single-probe kernels below take
+  // the table too: evaluated inline on the 16 SMs of a cluster it costs more
+  // than the table launch on all SMs - 128^2 x 20 slices on B200: 117 us
+  // inline against 83 + 9 us.)
   int trans_flag = ROW_TRANS;
   if (use_trans_table(p, n_probes, n_slices, n_draws) && build_trans_table(p, V, n_slices, n_draws, r, st) == WAP_OK) {
     r.ttab = p->ttab;
@@ -643,14 +652,13 @@ int fresnel_forward(wap_plan* p, const float* V, int n_slices, int n_draws, cons
   } else {
     clear_error();
   }
-  ColArgs c = base_col_args(p, H, H_lo);
-  c.psi = r.psi;
-  c.psi_bstride = plane;
-  c.dp = dp;
-  // one or two probes: every slice in one cooperative launch when the grid
-  // qualifies (wap_chain.cu), else one launch per pass below
+  // few probes: every slice in one launch when the grid qualifies - the wave
+  // held in a thread-block cluster (wap_cluster.cu), else a cooperative grid
+  // (wap_chain.cu) - else one launch per pass below
   if (!ckpt) {
-    const int rc2 = chain_forward(p, r, c, n_probes, n_slices, reinterpret_cast<float2*>(stack), st);
+    int rc2 = cluster_forward(p, r, c, n_probes, n_slices, reinterpret_cast<float2*>(stack), st);
+    if (rc2 != -1) return rc2;
+    rc2 = chain_forward(p, r, c, n_probes, n_slices, reinterpret_cast<float2*>(stack), st);
     if (rc2 != -1) return rc2;
   }
 

@@ -222,6 +222,7 @@ int chain_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes,
   int grid = 0;
   const ProfToken tok = prof_begin(WAP_KIND_ROW, st);
   if ((e = chain_launch(n, E, a, st, &grid)) != cudaSuccess) return cuda_fail(e, "chain_kernel");
+  p->chain_ran = 1;
   // one slice step: wave in / out twice, potential or table once
   prof_end(tok, st, (double)n_probes * n_slices * n * n * 20.0);
   return WAP_OK;
@@ -230,6 +231,13 @@ int chain_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes,
 }  // namespace wap
 
 using namespace wap;
+
+extern "C" int wap_plan_status_pending(wap_plan* p, int* pending) {
+  clear_error();
+  if (!p || !pending) return fail(WAP_ERR_ARG, "NULL argument");
+  *pending = p->chain_ran;
+  return WAP_OK;
+}
 
 extern "C" int wap_plan_status_async(wap_plan* p, int* host_status, void* stream) {
   clear_error();

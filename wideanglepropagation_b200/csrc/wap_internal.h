@@ -63,6 +63,12 @@ struct wap_plan {
   int chain_e = 0;
   unsigned* chain_count = nullptr;
   int* chain_status = nullptr;
+  int chain_ran = 0;                 // the last forward on this plan ran the chain kernel
+  // cluster kernel (wap_cluster.cu): its (n, E) twiddle table, and whether the
+  // device co-schedules a cluster of it (-1 not asked yet)
+  float4* cl_tw = nullptr;
+  int cl_e = 0;
+  int cl_fits = -1;
 };
 
 namespace wap {
@@ -104,6 +110,8 @@ int knob_value(int which);
 // plan or the call does not qualify (the caller then launches per pass)
 int chain_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes, int n_slices, float2* stack,
                   cudaStream_t st);
+int cluster_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probes, int n_slices, float2* stack,
+                    cudaStream_t st);
 
 // grids that are not powers of two (wap_generic.cu)
 bool generic_size_supported(int n);

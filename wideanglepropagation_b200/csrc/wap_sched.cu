@@ -1082,7 +1082,7 @@ static bool sched_size_ok(int n) { return n == 128 || n == 256 || n == 512 || n 
 // Scheduler overrides for A/B timing and tests (wap_scan_debug_override); -1:
 // the library's own choice.  Set only by an explicit call, never from the
 // environment, and read when a scan is created.
-static int g_knob[WAP_KNOB_COUNT] = {-1, -1, -1, -1, -1, -1, -1, -1};
+static int g_knob[WAP_KNOB_COUNT] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
 static int knob(int k) { return g_knob[k]; }
 namespace wap {
 int knob_value(int k) { return (k >= 0 && k < WAP_KNOB_COUNT) ? g_knob[k] : -1; }

@@ -95,7 +95,8 @@ def _to(x, dtype, device) -> torch.Tensor:
 
 
 # Recent splits of complex128 device tensors: (source tensor, its version,
-# device, hi, lo, event recorded after the split on the stream that made it).
+# device, hi, lo, event recorded after the split on the stream that made it,
+# that stream's handle).
 # An entry keeps its source alive, so no other tensor can take its memory
 # while cached, and an in-place change of the source bumps its version and
 # misses.  Inference tensors carry no version counter and are never cached.
@@ -132,22 +133,26 @@ def split_transfer(H, device, cache: bool = True):
         cacheable = ver is not None and t.device.type == "cuda" and t.device == dev
         if cacheable:
             with _split_lock:
-                for i, (src, sver, d, hi, lo, ev) in enumerate(_split_cache):
+                for i, (src, sver, d, hi, lo, ev, sid) in enumerate(_split_cache):
                     if src is t and sver == ver and d == dev:
                         _split_cache.append(_split_cache.pop(i))
                         cur = torch.cuda.current_stream(dev)
-                        cur.wait_event(ev)
-                        hi.record_stream(cur)
-                        lo.record_stream(cur)
+                        if cur.cuda_stream != sid:
+                            # made on another stream: wait for it, and keep the
+                            # halves' memory until this stream is done with it
+                            cur.wait_event(ev)
+                            hi.record_stream(cur)
+                            lo.record_stream(cur)
                         return hi, lo
         t = t.to(device)
         hi = t.to(torch.complex64).contiguous()
         lo = (t - hi.to(torch.complex128)).to(torch.complex64).contiguous()
         if cacheable:
+            cur = torch.cuda.current_stream(dev)
             ev = torch.cuda.Event()
-            ev.record(torch.cuda.current_stream(dev))
+            ev.record(cur)
             with _split_lock:
-                _split_cache.append((H, ver, dev, hi, lo, ev))
+                _split_cache.append((H, ver, dev, hi, lo, ev, cur.cuda_stream))
                 del _split_cache[:-_SPLIT_CACHE_MAX]
         return hi, lo
     return _to(t, torch.complex64, device), None
@@ -388,7 +393,8 @@ def _prepare(potential, probe, positions, draw, dev):
 
 SCAN_SIZES = (128, 256, 512, 1024)
 SCAN_MIN_PROBES = 8
-# forwards of at most this many probes on these square grids run as one cooperative launch
+# forwards of at most this many probes on these square grids run as one launch (a
+# cooperative grid, or a thread-block cluster per probe at 128)
 CHAIN_SIZES = (128, 256)
 CHAIN_MAX_PROBES = 2
 _scans: dict = {}
@@ -553,8 +559,10 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     position into one float32 pattern per position; exit waves stay per probe.
 
     Calls that run on the persistent scheduler (many probes of one probe) or
-    as one cooperative launch (one or two probes on a square 128 or 256 grid)
-    raise WapError if one of their bounded device-side waits expired; with
+    as one cooperative launch (one or two probes on a square 256 grid; on a
+    128 grid they run as one thread-block cluster per probe, without
+    device-side waits) raise WapError if one of their bounded device-side
+    waits expired; with
     ``check=False`` the call returns without waiting for the GPU and the
     failure is raised by ``check_errors()`` or by a later call.
     """
@@ -581,14 +589,15 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
     plan.set_detector(det)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
+    cur = torch.cuda.current_stream(dev)
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), _ptr(H), _ptr(H_lo), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
-        _ptr(stack), _stream()))
-    if B <= CHAIN_MAX_PROBES and ny == nx and ny in CHAIN_SIZES:
+        _ptr(stack), ctypes.c_void_p(cur.cuda_stream)))
+    if B <= CHAIN_MAX_PROBES and ny == nx and ny in CHAIN_SIZES and _lib.plan_status_pending(plan.handle):
         # one or two probes ran as one cooperative launch whose grid-wide waits are bounded
         token = _lib.scan_status_begin(plan.handle, f"one-launch chain of {B} probe(s) on {ny}x{nx}, {N} slices",
-                                       source="wap_plan_status_async")
+                                       source="wap_plan_status_async", stream=cur)
         if check:
             _lib.scan_status_end(token)
         else:
