@@ -66,6 +66,9 @@ def parse():
                     help="WPM case for ncu captures: C3 (512^2, K=16, plane wave) at 3 slices, two calls")
     ap.add_argument("--profile-single", action="store_true",
                     help="single-probe case for ncu captures: C2 (1024^2 AS, plane wave) at 10 slices, two calls")
+    ap.add_argument("--profile-cluster", action="store_true",
+                    help="cluster-kernel case for ncu captures: one Fresnel probe on 128^2, 20 slices (C1's slice "
+                         "count and probe on the grid the cluster kernel serves), two calls")
     ap.add_argument("--table", action="store_true",
                     help="per-configuration table (C1 Fresnel 256^2, C2 AS 1024^2, C3 WPM 512^2; one probe): B200 "
                          "time, CPU FP64/FP32 restatement on a bounded sample, error vs the FP64 oracle at full "
@@ -228,6 +231,9 @@ def main():
         return
     if args.profile_single:
         profile_single()
+        return
+    if args.profile_cluster:
+        profile_cluster()
         return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
@@ -405,14 +411,26 @@ def main():
 
 
 def _sources_sha256():
-    """Digest of the library's CUDA sources and C header (the build a profile
-    was taken on)."""
-    import glob
+    """Digest of the scan kernel's translation unit: wap_sched.cu and every
+    header it includes, followed recursively (the build a profile of that
+    kernel was taken on)."""
     import hashlib
+    import re
+    csrc = os.path.join(ROOT, "wideanglepropagation_b200", "csrc")
+    seen, order = set(), []
+
+    def visit(path):
+        path = os.path.normpath(path)
+        if path in seen or not os.path.exists(path):
+            return
+        seen.add(path)
+        order.append(path)
+        for inc in re.findall(r'^#include "([^"]+)"', open(path).read(), re.M):
+            visit(os.path.join(os.path.dirname(path), inc))
+
+    visit(os.path.join(csrc, "wap_sched.cu"))
     h = hashlib.sha256()
-    files = sorted(glob.glob(os.path.join(ROOT, "wideanglepropagation_b200", "csrc", "*"))) + \
-        [os.path.join(ROOT, "include", "wap.h")]
-    for f in files:
+    for f in sorted(order, key=os.path.basename):
         h.update(os.path.basename(f).encode())
         h.update(open(f, "rb").read())
     return h.hexdigest()
@@ -498,6 +516,21 @@ def profile_single():
         wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
     torch.cuda.synchronize()
     print(json.dumps({"profile_single": "ok"}))
+
+
+def profile_cluster():
+    import torch
+    import wideanglepropagation_b200 as wap
+    w = wap.synthetic.plain_fresnel(0)
+    n = 128
+    dev = torch.device("cuda", 0)
+    V = torch.as_tensor(w.potential[0][:, :n, :n].copy(), device=dev)
+    pr = torch.as_tensor(wap.synthetic.aperture_probe(n, n, w.ps, w.energy, 20.0, -30.0), device=dev)
+    H = wap.fresnel_propagation_kernel(n, n, (w.ps, w.ps), w.dz, w.energy)
+    for _ in range(2):
+        wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_cluster": "ok"}))
 
 
 def baseline_table():
