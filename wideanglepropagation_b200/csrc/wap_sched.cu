@@ -1141,10 +1141,11 @@ static int encode_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* map
 
 // Trailing checkpoint segments whose waves the forward keeps, so that the
 // backward recomputes none of them: memory stays O(sqrt N) - checkpoints every
-// k slices plus 3k waves - and three segments' recompute (2k - 1 passes each)
+// k slices plus 4k waves - and four segments' recompute (2k - 1 passes each)
 // drop.  Two kept segments left the 512^2 x 64-slice gradient step at 3.03 x
-// its forward after the forward scan itself had become faster.
-constexpr int kKeptSegments = 3;
+// its forward after the forward scan itself had become faster, three at
+// 2.93 - 2.98, four at 2.83 - 2.87 (B200, the same box).
+constexpr int kKeptSegments = 4;
 
 static int kept_first_slice(int n_slices, int k) {
   const int nck = (n_slices + k - 1) / k;
