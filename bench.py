@@ -80,6 +80,8 @@ def parse():
                          "counts with fewer probes (228 on 256^2 = two probe groups of 114, 32 on 512^2 = one "
                          "group), one warm-up and one step, no extras; the library's bytes per pixel-slice-step "
                          "are the same per probe group as in the full step")
+    ap.add_argument("--class-only", type=int, default=0, choices=[0, 256, 512],
+                    help="with --traffic-case: keep only the class of this grid size (per-class profiles)")
     ap.add_argument("--profile-case", action="store_true",
                     help="reduced scan for ncu captures: 512 probes 256^2 x 4 slices + 32 probes 512^2 x 4 "
                          "slices (waves 256 + 64 MB, above L2), one warm-up and one step, no extras")
@@ -247,6 +249,8 @@ def main():
                                             draw_of_probe=full[0].draw_of_probe[:228]),
                         dataclasses.replace(full[1], positions=full[1].positions[:32],
                                             draw_of_probe=full[1].draw_of_probe[:32])]
+        if args.class_only:
+            classes_host = [w for w in classes_host if w.ny == args.class_only]
         args.steps, args.warmup, args.no_extras = 1, 1, True
     else:
         classes_host = S.batched_scan(0, small=args.small)

@@ -321,6 +321,9 @@ struct RowExchange {
   float2* base;
   __device__ __forceinline__ void st(int p, float2 v) const { base[p + (p >> 4)] = v; }
   __device__ __forceinline__ float2 ld(int p) const { return base[p + (p >> 4)]; }
+  // position b + o, b a run-time value and o a compile-time offset
+  __device__ __forceinline__ void st2(int b, int o, float2 v) const { st(b + o, v); }
+  __device__ __forceinline__ float2 ld2(int b, int o) const { return ld(b + o); }
   __device__ __forceinline__ void sync() const {
     if constexpr (WARP_LOCAL) __syncwarp();
     else block_sync<BAR, NT>();
@@ -336,6 +339,28 @@ struct ColExchange {
   int w, c;
   __device__ __forceinline__ void st(int p, float2 v) const { base[p * w + c] = v; }
   __device__ __forceinline__ float2 ld(int p) const { return base[p * w + c]; }
+  __device__ __forceinline__ void st2(int b, int o, float2 v) const { st(b + o, v); }
+  __device__ __forceinline__ float2 ld2(int b, int o) const { return ld(b + o); }
+  __device__ __forceinline__ void sync() const { block_sync<BAR, NT>(); }
+};
+
+// ColExchange with one padding row per 16: position p lives in row
+// p + p / 16 of a [N + N/16][W] buffer.  With W = 8 (512-point columns) the
+// radix-16 scatter of the first stage sends the two positions 16 rows apart
+// that a half-warp stores to the same banks of an unpadded [N][8] tile; the
+// padding row moves every other 16-row block to the other half of the banks.
+// The padded row is formed from the stage's run-time base b and compile-time
+// offset o separately - pad(b + o) = pad(b) + pad(o) - which holds when the
+// low four bits of b and o do not carry: true of every E = 16 Stockham stage
+// (first stage: b a multiple of 16, o < 16; later stages and the reads: o a
+// multiple of 16).
+template <int BAR = 0, int NT = 0>
+struct ColExchangePad {
+  float2* base;
+  int w, c;
+  __device__ __forceinline__ static int pad(int p) { return p + (p >> 4); }
+  __device__ __forceinline__ void st2(int b, int o, float2 v) const { base[(pad(b) + pad(o)) * w + c] = v; }
+  __device__ __forceinline__ float2 ld2(int b, int o) const { return base[(pad(b) + pad(o)) * w + c]; }
   __device__ __forceinline__ void sync() const { block_sync<BAR, NT>(); }
 };
 
@@ -376,11 +401,11 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], int t, const X& xs, co
       const int k = b & (L - 1);
       const int base = (b - k) * R + k;
 #pragma unroll
-      for (int m = 0; m < R; ++m) xs.st(base + m * L, v[q + B * m]);
+      for (int m = 0; m < R; ++m) xs.st2(base, m * L, v[q + B * m]);
     }
     xs.sync();
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
+    for (int e = 0; e < E; ++e) v[e] = xs.ld2(t, T * e);
   }
 }
 

@@ -491,7 +491,15 @@ __device__ __forceinline__ void col_compute(const SchedClass& c, const Task& k, 
   const int cc = threadIdx.x % W, t = threadIdx.x / W;
   const int col = k.tile * W + cc;
   const long long plane = (long long)N * N;
-  const ColExchange<kFftBar, kSchedThreads> xs{exch, W, cc};
+  // 512-point columns (8 per tile) exchange through the padded tile: the
+  // unpadded one costs the first stage's scatter a 2-way bank conflict
+  // (B200, 512^2 scan: 14 % of its shared-memory wavefronts); its
+  // (512 + 32) x 8 entries fill the exchange buffer exactly
+  using XS = typename std::conditional<N == 512 && E == 16, ColExchangePad<kFftBar, kSchedThreads>,
+                                       ColExchange<kFftBar, kSchedThreads>>::type;
+  static_assert(N != 512 || E != 16 || (N + N / 16) * W * sizeof(float2) <= kExchBytesFor(16),
+                "padded 512-point column tile fits the exchange buffer");
+  const XS xs{exch, W, cc};
   const int type = st.type;
   fft<N, E, false>(v, t, xs, tw);
   const int sx = (col + (N >> 1)) & (N - 1);
