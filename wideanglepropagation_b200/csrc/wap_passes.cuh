@@ -643,11 +643,12 @@ wpm_col_kernel(const WpmColArgs a) {
   const long long plane = (long long)NY * nx;
   const ColExchange<> xs{tile, W, c};
 
+  // the column straight from global memory (a warp reads W consecutive
+  // columns of each of its rows; the tile serves the transforms only)
   float2 v[E];
-  tile_load<NY>(tile, a.psi + (long long)b * plane + (long long)blockIdx.x * W, W, nx);
-  __syncthreads();
+  const float2* pcol = a.psi + (long long)b * plane + col;
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
+  for (int e = 0; e < E; ++e) v[e] = __ldcg(pcol + (long long)(t + T * e) * nx);
   fft<NY, E, false>(v, t, xs, tw);
 
   if (a.dp_mode) {
@@ -684,7 +685,7 @@ wpm_col_kernel(const WpmColArgs a) {
     pa[e] = q0[e] > 0.0f ? 0.5f * a.dz * sqrtf(pr[e]) : 0.0f;
   }
 
-  float2* ftile = a.fields + (long long)b * a.K * plane + (long long)blockIdx.x * W;
+  float2* fcol = a.fields + (long long)b * a.K * plane + col;
   const int kb = blockIdx.z * a.kpg, ke = min(kb + a.kpg, a.K);
   for (int k = kb; k < ke; ++k) {
     const float dk = srefs[k];
@@ -701,11 +702,11 @@ wpm_col_kernel(const WpmColArgs a) {
       u[e] = wpm_bin_direct(v[e], pr[e], ak, a.dz, a.hvac + (long long)(t + T * e) * nx + col);
     }
     fft<NY, E, true>(u, t, xs, tw);
-    __syncthreads();
+    // field k straight from the registers (no staging through the tile: the
+    // next transform's first exchange waits for every thread's reads)
+    float2* fk = fcol + (long long)k * plane;
 #pragma unroll
-    for (int e = 0; e < E; ++e) xs.st(t + T * e, u[e]);
-    __syncthreads();
-    tile_store<NY>(ftile + (long long)k * plane, tile, W, nx);
+    for (int e = 0; e < E; ++e) __stcg(fk + (long long)(t + T * e) * nx, u[e]);
   }
 }
 
