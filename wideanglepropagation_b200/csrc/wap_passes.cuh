@@ -358,12 +358,15 @@ __device__ __forceinline__ void col_pass_body(const ColArgs& a, const float4* tw
   const int b = a.probe0 + by;
   const int nx = a.nx;
   const long long plane = (long long)NY * nx;
-  float2* ptile = a.psi + (long long)b * a.psi_bstride + (long long)bx * W;
+  // the column straight between global memory and registers (a warp moves W
+  // consecutive columns of each of its rows; the tile serves the transforms)
+  float2* pcol = a.psi + (long long)b * a.psi_bstride + col;
   const ColExchange<> xs{tile, W, c};
   const int f = a.flags;
 
   float2 v[E];
-  tile_load<NY>(tile, ptile, W, nx);
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = __ldcg(pcol + (long long)(t + T * e) * nx);
   // short-chain shapes fetch H (hi and lo) before the forward transform, as
   // the row pass does with the transmission
   constexpr bool kEarlyH = E <= 8;
@@ -376,9 +379,6 @@ __device__ __forceinline__ void col_pass_body(const ColArgs& a, const float4* tw
       lpre[e] = a.H_lo ? __ldg(a.H_lo + o) : make_float2(0.f, 0.f);
     }
   }
-  __syncthreads();
-#pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = xs.ld(t + T * e);
 
   if (!(f & COL_NO_FFT)) fft<NY, E, false>(v, t, xs, tw);
 
@@ -455,12 +455,8 @@ __device__ __forceinline__ void col_pass_body(const ColArgs& a, const float4* tw
   }
 
   if (!(f & COL_FWD_ONLY)) fft<NY, E, true>(v, t, xs, tw);
-
-  __syncthreads();
 #pragma unroll
-  for (int e = 0; e < E; ++e) xs.st(t + T * e, v[e]);
-  __syncthreads();
-  tile_store<NY>(ptile, tile, W, nx);
+  for (int e = 0; e < E; ++e) __stcg(pcol + (long long)(t + T * e) * nx, v[e]);
 }
 
 template <int NY, int E, bool SEED>
