@@ -316,9 +316,11 @@ row_pass_kernel(const RowArgs a) {
 }
 
 // ----------------------------------------------------------------------------
-// column tiles: [NY][W] complex64 between global memory (row stride nx) and
+// column tile load: [NY][W] complex64 from global memory (row stride nx) into
 // shared memory, 16 bytes per access; consecutive threads take consecutive
-// 16-byte words of a row segment, so a warp moves 512 contiguous-by-row bytes.
+// 16-byte words of a row segment, so a warp moves 512 contiguous-by-row bytes
+// (the adjoint seed's second input; the column passes themselves move their
+// columns between registers and global memory directly)
 // ----------------------------------------------------------------------------
 template <int NY>
 __device__ __forceinline__ void tile_load(float2* tile, const float2* __restrict__ g, int W, int nx) {
@@ -328,17 +330,6 @@ __device__ __forceinline__ void tile_load(float2* tile, const float2* __restrict
   for (int i = threadIdx.x; i < NY * w2; i += blockDim.x) {
     const int r = i >> sh, c2 = i & (w2 - 1);
     t4[i] = __ldcg(reinterpret_cast<const float4*>(g + (long long)r * nx) + c2);
-  }
-}
-
-template <int NY>
-__device__ __forceinline__ void tile_store(float2* __restrict__ g, const float2* tile, int W, int nx) {
-  const int w2 = W >> 1;
-  const int sh = __ffs(w2) - 1;
-  const float4* t4 = reinterpret_cast<const float4*>(tile);
-  for (int i = threadIdx.x; i < NY * w2; i += blockDim.x) {
-    const int r = i >> sh, c2 = i & (w2 - 1);
-    __stcg(reinterpret_cast<float4*>(g + (long long)r * nx) + c2, t4[i]);
   }
 }
 
