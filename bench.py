@@ -542,7 +542,11 @@ def baseline_table():
     API (inputs resident, no wavefront stack), error vs the FP64 oracle on
     the full configuration, the oracle in FP64 and FP32 on the host cores
     (best of 3 after a warm-up, reduced slice counts, per slice-step), and the
-    roofline fraction at 20 B per pixel-slice-step."""
+    roofline fraction: the roofline time max(bytes / HBM peak, flops / FP32
+    peak) over the measured time, with 20 B per pixel-slice-step and the
+    flops 10 N log2 N + 24 N per slice-step (Fresnel / AS) or
+    (K + 1) 5 N log2 N + 30 K N (WPM), N the pixels of the grid; the HBM and
+    FP32 fractions beside it."""
     import torch
     import wideanglepropagation_b200 as wap
     from oracle import propagation_oracle as O
@@ -551,6 +555,7 @@ def baseline_table():
     cores = os.cpu_count() or 1
     O.set_workers(cores)
     peak, src = _peak_hbm()
+    fp32 = _fp32_peak()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def timeit(fn, reps):
@@ -596,14 +601,22 @@ def baseline_table():
                    for m in ("fp64", "fp32")}
         ms = timeit(gpu, 20 if kind == "fresnel" else 5 if kind == "as" else 2)
         ex, dp, _ = gpu()
+        npx = w.ny * w.nx
+        flops = w.n_slices * ((w.n_bins + 1) * 5.0 * npx * np.log2(npx) + 30.0 * w.n_bins * npx if kind == "wpm"
+                              else 10.0 * npx * np.log2(npx) + 24.0 * npx)
+        t_bytes = 20.0 * npx * w.n_slices / (peak * 1e9)
+        t_flops = flops / (fp32 * 1e12)
         rows[name] = {
             "gpu_ms_per_call": ms, "gpu_slice_steps_per_s": w.n_slices / (ms / 1e3),
-            "roofline_frac": 20.0 * w.ny * w.nx * w.n_slices / (ms / 1e3) / 1e9 / peak,
+            "roofline_frac": max(t_bytes, t_flops) / (ms / 1e3),
+            "roofline_bound": "hbm" if t_bytes >= t_flops else "fp32",
+            "hbm_frac": t_bytes / (ms / 1e3), "fp32_frac": t_flops / (ms / 1e3),
             "err_vs_fp64_exit": float(O.rel_l2(ex.cpu().numpy(), ref[0])),
             "err_vs_fp64_dp": float(O.rel_l2(dp.cpu().numpy(), ref[1])),
             "cpu_fp64_slice_steps_per_s": cpu["fp64"], "cpu_fp32_slice_steps_per_s": cpu["fp32"],
             "cpu_sample_slices": cpu_slices, "cores": cores}
-    print(json.dumps({"table": rows, "peak_gbs": peak, "peak_source": src}), flush=True)
+    print(json.dumps({"table": rows, "peak_gbs": peak, "peak_source": src, "fp32_tflops": fp32,
+                      "fp32_source": "FMA probe (wap_fp32_probe) in this run"}), flush=True)
 
 
 def _wall(fn):
