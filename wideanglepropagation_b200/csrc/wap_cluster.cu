@@ -257,8 +257,9 @@ static cudaError_t cluster_launch_t(const ClusterArgs& a, int n_probes, cudaStre
     *fits = clusters >= 1;
     return cudaSuccess;
   }
-  count_launch();
-  return cudaLaunchKernelEx(&cfg, kern, a);
+  const cudaError_t r = cudaLaunchKernelEx(&cfg, kern, a);
+  if (r == cudaSuccess) count_launch();
+  return r;
 }
 
 // elements per thread of the cluster kernel: 128 threads per CTA at 128^2
@@ -318,7 +319,17 @@ int cluster_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probe
   a.tw = p->cl_tw;
   bool fits = true;
   const ProfToken tok = prof_begin(WAP_KIND_ROW, st);
-  if ((e = cluster_launch(n, E, a, n_probes, st, true, &fits)) != cudaSuccess) return cuda_fail(e, "cluster_kernel");
+  if ((e = cluster_launch(n, E, a, n_probes, st, true, &fits)) != cudaSuccess) {
+    // a device shared with other work may refuse the 16-CTA cluster at launch
+    // even where the occupancy query allowed it: the chain serves this plan
+    // from now on (a refused launch leaves no error behind)
+    if (e == cudaErrorInvalidClusterSize || e == cudaErrorLaunchOutOfResources) {
+      cudaGetLastError();
+      p->cl_fits = 0;
+      return -1;
+    }
+    return cuda_fail(e, "cluster_kernel");
+  }
   // one slice step: wave in / out twice, potential or table once
   prof_end(tok, st, (double)n_probes * n_slices * n * n * 20.0);
   return WAP_OK;
