@@ -342,8 +342,10 @@ int wap_scan_debug_checks(wap_scan* scan, int on, int* record);
  *                      waits, 0: none (the default)
  *   WAP_KNOB_H_HI      reserved
  *   WAP_KNOB_CLUSTER   0: single-probe forwards without the cluster kernel
- *                      (wave in distributed shared memory); 4 / 8 / 16 that
- *                      many elements per thread */
+ *                      (wave in distributed shared memory); 1: its launch
+ *                      counts as refused by the device without being issued
+ *                      (the plan falls back to the chain kernel for good);
+ *                      4 / 8 / 16 that many elements per thread */
 #define WAP_KNOB_ELEMS 0
 #define WAP_KNOB_TWIDDLES 1
 #define WAP_KNOB_TW_SMEM 2

@@ -117,3 +117,39 @@ def test_cluster_repeatable(wap):
     chain = _with({_lib.WAP_KNOB_CLUSTER: 0},
                   lambda: wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)[0])
     assert rel(outs[0].cpu().numpy(), chain.cpu().numpy()) < 2e-6
+
+
+def test_refused_cluster_launch_falls_back_to_chain(wap):
+    """A cluster launch that the device refuses (injected on the host: knob
+    value 1 makes the call treat the launch as refused without issuing it)
+    leaves no error behind: the call runs on the chain kernel, bit for bit the
+    chain's result, and so does every later call of that plan."""
+    V, probe, ps, dz, E = _setup(128, 9, seed=21)
+    H = wap.angular_spectrum_propagation_kernel(128, 128, (ps, ps), dz, E)
+    call = lambda: wap.simulate_fresnel_as(V, probe, H, dz, E, return_wavefronts=False)
+
+    def counted():
+        l0 = _lib.launch_count()
+        out = call()
+        torch.cuda.synchronize()
+        return out, _lib.launch_count() - l0
+    # whether the plan's last forward ran the chain kernel (it then has a status word to read)
+    chain_ran = lambda: _lib.plan_status_pending(
+        wap.propagation.get_plan(128, 128, 1, _lib.WAP_OP_FRESNEL_AS).handle)
+    wap.release_caches()   # a plan of its own: the fallback is kept for the plan's life
+    try:
+        call()
+        assert not chain_ran()   # the default: the cluster kernel
+        (chain, _, _), _ = _with({_lib.WAP_KNOB_CLUSTER: 0}, counted)
+        assert chain_ran()
+        (ex, dp, _), launches = _with({_lib.WAP_KNOB_CLUSTER: 1}, counted)
+        assert chain_ran()
+        assert 1 <= launches <= 2, launches   # [transmission table +] the chain kernel, not the refused one
+        assert torch.equal(ex, chain)
+        (ex2, _, _), launches = counted()   # knob back to the default: the plan stays on the chain
+        assert chain_ran()
+        assert 1 <= launches <= 2, launches
+        assert torch.equal(ex2, chain)
+        wap.check_errors()
+    finally:
+        wap.release_caches()

@@ -171,7 +171,7 @@ def test_api_raises_on_scheduler_timeout(wap):
     ex0, _, _ = wap.simulate_fresnel_as(*args, **kw)
     torch.cuda.synchronize()
     key = (torch.cuda.current_device(), 128, host.n_slices, 1, host.n_probes)
-    h = P._scans[key]
+    h, _ = P._scans[key]   # (scan handle, StreamOrder)
     L = _lib.lib()
     try:
         _lib.check(L.wap_scan_debug_stall(h, 1, 1 << 12))

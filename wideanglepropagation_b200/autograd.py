@@ -24,11 +24,12 @@ import ctypes
 import threading
 
 from . import _lib
-from .propagation import (SCAN_MIN_PROBES, SCAN_SIZES, _detector, _device, _dp_shape, _prepare, _ptr, _stream,
+from .propagation import (SCAN_MIN_PROBES, SCAN_SIZES, StreamOrder, _detector, _device, _dp_shape, _prepare, _ptr,
                           get_plan, scan_class, split_transfer)
 
-# gradient scans (persistent scheduler) by shape; a scan is held from the
-# forward until its backward has run, so several pending graphs get their own
+# gradient scans (persistent scheduler) by shape, each with the StreamOrder of
+# its workspace; a scan is held from the forward until its backward has run,
+# so several pending graphs get their own
 _pool: dict = {}
 _pool_lock = threading.Lock()
 
@@ -40,22 +41,22 @@ def _acquire(key, cls, k):
     with _pool_lock:
         free = _pool.setdefault(key, [])
         if free:
-            h = free.pop()
+            h, order = free.pop()
             _lib.check(L.wap_scan_bind(h, 1, ptr))
-            return h
+            return h, order
     h = ctypes.c_void_p()
     _lib.check(L.wap_scan_grad_create(ctypes.byref(h), ptr, int(k)))
-    return h
+    return h, StreamOrder()
 
 
 _POOL_IDLE_MAX = 2   # idle gradient scans kept per shape (each holds its checkpoints and segment waves)
 
 
-def _release(key, h):
+def _release(key, h, order):
     with _pool_lock:
         free = _pool.setdefault(key, [])
         if len(free) < _POOL_IDLE_MAX:
-            free.append(h)
+            free.append((h, order))
             return
     _lib.lib().wap_scan_destroy(h)
 
@@ -63,7 +64,7 @@ def _release(key, h):
 def release_pool() -> None:
     """Destroy every idle pooled gradient scan (scans held by pending graphs stay)."""
     with _pool_lock:
-        handles = [h for free in _pool.values() for h in free]
+        handles = [h for free in _pool.values() for h, _ in free]
         _pool.clear()
     if handles:
         torch.cuda.synchronize()
@@ -75,13 +76,13 @@ class _Lease:
     """A pooled gradient scan held by one forward: returned to the pool by
     its backward, or when the graph is freed without a backward."""
 
-    def __init__(self, key, h):
-        self.key, self.h, self.done = key, h, False
+    def __init__(self, key, h, order):
+        self.key, self.h, self.order, self.done = key, h, order, False
 
     def release(self):
         if not self.done:
             self.done = True
-            _release(self.key, self.h)
+            _release(self.key, self.h, self.order)
 
     def __del__(self):
         self.release()
@@ -101,11 +102,14 @@ class MultisliceFunction(torch.autograd.Function):
             dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
             k = max(1, min(int(ckpt_every), N))
             key = (torch.cuda.current_device(), ny, N, Vc.shape[0], B, k)
-            h = _acquire(key, scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp, det), k)
-            _lib.check(_lib.lib().wap_scan_run(h, _stream()))
-            ctx.scan = _Lease(key, h)
+            h, order = _acquire(key, scan_class(Vc, psi, pos, dr, Hc, Hl, dz, energy, exit_wave, dp, det), k)
+            ctx.scan = _Lease(key, h, order)
+            cur = order.begin(torch.cuda.current_stream(dev))
+            _lib.check(_lib.lib().wap_scan_run(h, ctypes.c_void_p(cur.cuda_stream)))
             ctx.check = check
-            token = _lib.scan_status_begin(h, f"gradient scan forward of {B} probes on {ny}x{nx}, {N} slices")
+            token = _lib.scan_status_begin(h, f"gradient scan forward of {B} probes on {ny}x{nx}, {N} slices",
+                                           stream=cur)
+            order.end(cur)
             if check:
                 _lib.scan_status_end(token)
             else:
@@ -127,10 +131,12 @@ class MultisliceFunction(torch.autograd.Function):
         exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
         dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
         ckpt = torch.empty((B, nck, ny, nx), dtype=torch.complex64, device=dev)
+        cur = plan.begin()
         _lib.check(_lib.lib().wap_multislice_fwd_ckpt(
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
             _ptr(pos), _ptr(Hc), _ptr(Hl), float(dz), float(energy), _ptr(exit_wave), _ptr(dp), _ptr(ckpt), k,
-            _stream()))
+            ctypes.c_void_p(cur.cuda_stream)))
+        plan.end(cur)
         empty = torch.empty(0, device=dev)
         ctx.save_for_backward(Vc, Hc, Hl if Hl is not None else empty, exit_wave, ckpt,
                               dr if dr is not None else empty)
@@ -151,10 +157,12 @@ class MultisliceFunction(torch.autograd.Function):
                     return grad_V.reshape(vshape), None, None, None, None, None, None, None, None, None
                 g = None if g_dp is None else g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
                 ge = None if g_exit is None else g_exit.to(torch.complex64).reshape(B, ny, nx).contiguous()
+                cur = lease.order.begin(torch.cuda.current_stream(Vc.device))
                 _lib.check(_lib.lib().wap_scan_grad_backward_ex(lease.h, _ptr(g), _ptr(ge), _ptr(grad_V),
-                                                                _stream()))
+                                                                ctypes.c_void_p(cur.cuda_stream)))
                 token = _lib.scan_status_begin(lease.h, f"gradient scan backward of {B} probes on {ny}x{nx}, "
-                                                        f"{N} slices")
+                                                        f"{N} slices", stream=cur)
+                lease.order.end(cur)
                 if ctx.check:
                     _lib.scan_status_end(token)
                 else:
@@ -173,10 +181,13 @@ class MultisliceFunction(torch.autograd.Function):
             g_dp = g_dp.to(torch.float32).reshape(_dp_shape(B, ny, nx, det)).contiguous()
         grad_V = torch.zeros(Vc.shape, dtype=torch.float32, device=dev)
         work = torch.empty((B, k + 2, ny, nx), dtype=torch.complex64, device=dev)
+        cur = plan.begin()
         _lib.check(_lib.lib().wap_multislice_bwd(
             plan.handle, _ptr(Vc), N, Vc.shape[0], _ptr(dr) if has_draw else None, B, _ptr(Hc),
             _ptr(Hl) if Hl.numel() else None, dz, energy,
-            _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work), _stream()))
+            _ptr(exit_wave), _ptr(ckpt), k, _ptr(g_dp), _ptr(g_exit), _ptr(grad_V), _ptr(work),
+            ctypes.c_void_p(cur.cuda_stream)))
+        plan.end(cur)
         return grad_V.reshape(vshape), None, None, None, None, None, None, None, None, None
 
 

@@ -319,12 +319,16 @@ int cluster_forward(wap_plan* p, const RowArgs& r, const ColArgs& c, int n_probe
   a.tw = p->cl_tw;
   bool fits = true;
   const ProfToken tok = prof_begin(WAP_KIND_ROW, st);
-  if ((e = cluster_launch(n, E, a, n_probes, st, true, &fits)) != cudaSuccess) {
+  // knob value 1: the launch counts as refused without being issued (a
+  // host-side test of the fallback below)
+  e = kv == 1 ? cudaErrorInvalidClusterSize : cluster_launch(n, E, a, n_probes, st, true, &fits);
+  if (e != cudaSuccess) {
+    prof_end(tok, st, 0.0);   // closes the trace token (a record of zero bytes)
     // a device shared with other work may refuse the 16-CTA cluster at launch
     // even where the occupancy query allowed it: the chain serves this plan
     // from now on (a refused launch leaves no error behind)
     if (e == cudaErrorInvalidClusterSize || e == cudaErrorLaunchOutOfResources) {
-      cudaGetLastError();
+      if (kv != 1) cudaGetLastError();
       p->cl_fits = 0;
       return -1;
     }

@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .propagation import _device, _ptr, _stream, _to, get_plan, split_transfer
+from .propagation import _device, _ptr, _to, get_plan, split_transfer
 
 __all__ = ["build_lippmann_schwinger_kernel_2d", "apply_convolution", "solve_scattering_2d_lippmann_schwinger"]
 
@@ -74,9 +74,11 @@ class _Convolution:
         plan = get_plan(self.Ex, self.Ey, 1, _lib.WAP_OP_FRESNEL_AS)
         self.src.zero_()
         self.src[self.sx:self.sx + self.Nx, self.sy:self.sy + self.Ny] = source
+        cur = plan.begin()
         _lib.check(_lib.lib().wap_multislice_fwd(
             plan.handle, _ptr(self.V0), 1, 1, None, _ptr(self.src), 1, 0, None, _ptr(self.Kh), _ptr(self.Kl),
-            1.0, 1.0e5, _ptr(self.out), None, None, _stream()))
+            1.0, 1.0e5, _ptr(self.out), None, None, ctypes.c_void_p(cur.cuda_stream)))
+        plan.end(cur)
         return self.out[self.sx:self.sx + self.Nx, self.sy:self.sy + self.Ny]
 
 

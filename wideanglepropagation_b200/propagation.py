@@ -124,13 +124,16 @@ def split_transfer(H, device, cache: bool = True):
     A complex128 tensor already on the device is split once and reused while
     it is unchanged (a transfer function normally serves many calls); a caller
     on another stream than the one that made the split waits for it first.
-    ``cache=False`` (internal scratch that the kernels rewrite) always splits.
+    ``cache=False`` (internal scratch that the kernels rewrite) always splits,
+    and so does a call inside a CUDA graph capture (the split becomes part of
+    the graph: the cache's events cannot cross the capture boundary).
     """
     t = H if isinstance(H, torch.Tensor) else torch.as_tensor(np.asarray(H))
     if t.dtype == torch.complex128:
         dev = torch.device(device)
         ver = _version_of(t) if cache else None
-        cacheable = ver is not None and t.device.type == "cuda" and t.device == dev
+        cacheable = (ver is not None and t.device.type == "cuda" and t.device == dev
+                     and not torch.cuda.is_current_stream_capturing())
         if cacheable:
             with _split_lock:
                 for i, (src, sver, d, hi, lo, ev, sid) in enumerate(_split_cache):
@@ -175,8 +178,43 @@ def _pair(ps) -> tuple:
     return ps
 
 
+class StreamOrder:
+    """Stream order of one cached native object (a plan or a scan: device
+    workspace that every call reuses).  It remembers the stream of the last
+    use; a use from another stream first waits for everything issued on that
+    stream so far (an event recorded there at the switch), so that calls on
+    different CUDA streams never run on the same workspace at once.  Uses on
+    one stream are ordered by the stream itself and cost nothing here.  A use
+    inside a CUDA graph capture does not wait (a dependency on work outside
+    the capture is not allowed there): a captured graph is ordered by the
+    stream it is replayed on, like any graph.  If the last stream can no
+    longer take an event (a caller's external stream, destroyed since), the
+    switch waits for the whole device instead."""
+
+    __slots__ = ("last",)
+
+    def __init__(self):
+        self.last = None
+
+    def begin(self, cur):
+        last = self.last
+        if last is not None and last.cuda_stream != cur.cuda_stream \
+                and not torch.cuda.is_current_stream_capturing():
+            try:
+                ev = torch.cuda.Event()
+                ev.record(last)
+                cur.wait_event(ev)
+            except RuntimeError:
+                torch.cuda.synchronize(cur.device)
+        return cur
+
+    def end(self, cur) -> None:
+        self.last = cur
+
+
 class Plan:
-    """Owns one ``wap_plan`` (twiddle tables, WPM workspace) on one device."""
+    """Owns one ``wap_plan`` (twiddle tables, WPM workspace) on one device;
+    ``order`` keeps its uses from different streams apart."""
 
     def __init__(self, ny: int, nx: int, max_batch: int, op: int, n_bins: int = 0):
         L = _lib.lib()
@@ -186,6 +224,14 @@ class Plan:
         self.ny, self.nx, self.max_batch, self.op, self.n_bins = ny, nx, max_batch, op, n_bins
         self.device = torch.cuda.current_device()
         self.det = None
+        self.order = StreamOrder()
+
+    def begin(self):
+        """The current stream, after the plan's last use on another stream."""
+        return self.order.begin(torch.cuda.current_stream(self.device))
+
+    def end(self, cur) -> None:
+        self.order.end(cur)
 
     def set_config(self, row_e: int, col_e: int, col_w: int) -> None:
         _lib.check(_lib.lib().wap_plan_set_config(self.handle, row_e, col_e, col_w))
@@ -397,7 +443,7 @@ SCAN_MIN_PROBES = 8
 # cooperative grid, or a thread-block cluster per probe at 128)
 CHAIN_SIZES = (128, 256)
 CHAIN_MAX_PROBES = 2
-_scans: dict = {}
+_scans: dict = {}          # key -> (scan handle, StreamOrder)
 _scans_lock = threading.Lock()
 
 
@@ -501,15 +547,18 @@ def _scan_run(V, psi, pos, dr, H, H_lo, dz, energy, exit_wave, dp, det=None, che
     L = _lib.lib()
     arr = ctypes.cast(cls, ctypes.c_void_p)
     with _scans_lock:
-        h = _scans.get(key)
-        if h is None:
+        ent = _scans.get(key)
+        if ent is None:
             h = ctypes.c_void_p()
             _lib.check(L.wap_scan_create(ctypes.byref(h), 1, arr))
-            _scans[key] = h
+            ent = _scans[key] = (h, StreamOrder())
         else:
-            _lib.check(L.wap_scan_bind(h, 1, arr))
-        _lib.check(L.wap_scan_run(h, _stream()))
-        token = _lib.scan_status_begin(h, f"persistent scan of {B} probes on {n}x{n}, {N} slices")
+            _lib.check(L.wap_scan_bind(ent[0], 1, arr))
+        h, order = ent
+        cur = order.begin(torch.cuda.current_stream(dev))
+        _lib.check(L.wap_scan_run(h, ctypes.c_void_p(cur.cuda_stream)))
+        token = _lib.scan_status_begin(h, f"persistent scan of {B} probes on {n}x{n}, {N} slices", stream=cur)
+        order.end(cur)
     if check:
         _lib.scan_status_end(token)
     else:
@@ -531,7 +580,7 @@ def release_caches() -> None:
     with _split_lock:
         _split_cache.clear()
     with _scans_lock:
-        for h in _scans.values():
+        for h, _ in _scans.values():
             _lib.lib().wap_scan_destroy(h)
         _scans.clear()
     with _plans_lock:
@@ -589,7 +638,7 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
     plan = get_plan(ny, nx, B, _lib.WAP_OP_FRESNEL_AS)
     plan.set_detector(det)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
-    cur = torch.cuda.current_stream(dev)
+    cur = plan.begin()
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), _ptr(H), _ptr(H_lo), float(slice_thickness), float(energy), _ptr(exit_wave), _ptr(dp),
@@ -598,10 +647,13 @@ def simulate_fresnel_as(potential, probe, prop_kernel, slice_thickness, energy, 
         # one or two probes ran as one cooperative launch whose grid-wide waits are bounded
         token = _lib.scan_status_begin(plan.handle, f"one-launch chain of {B} probe(s) on {ny}x{nx}, {N} slices",
                                        source="wap_plan_status_async", stream=cur)
+        plan.end(cur)
         if check:
             _lib.scan_status_end(token)
         else:
             _lib.defer_status(token)
+    else:
+        plan.end(cur)
     if accumulate is not None:
         dp = accumulate_patterns(dp, accumulate)
     if not batched:
@@ -641,10 +693,12 @@ def simulate_wpm(potential, probe, slice_thickness, energy, sampling, n_bins=128
     exit_wave = torch.empty((B, ny, nx), dtype=torch.complex64, device=dev)
     dp = torch.empty(_dp_shape(B, ny, nx, det), dtype=torch.float32, device=dev)
     stack = torch.empty((B, N, ny, nx), dtype=torch.complex64, device=dev) if return_wavefronts else None
+    cur = plan.begin()
     _lib.check(_lib.lib().wap_wpm_fwd(
         plan.handle, _ptr(V), N, V.shape[0], _ptr(dr), _ptr(psi), B, 1 if per_probe else 0,
         _ptr(pos), float(slice_thickness), float(energy), dy, dx, float(power_spacing),
-        _ptr(exit_wave), _ptr(dp), _ptr(stack), _stream()))
+        _ptr(exit_wave), _ptr(dp), _ptr(stack), ctypes.c_void_p(cur.cuda_stream)))
+    plan.end(cur)
     if accumulate is not None:
         dp = accumulate_patterns(dp, accumulate)
     if not batched:
@@ -685,11 +739,16 @@ def wpm_propagation_kernel_vmap(Ek, n_vals, k0, k_perp2, dz) -> torch.Tensor:
     out = torch.empty((nv.size, ny, nx), dtype=torch.complex64, device=dev)
     H = torch.empty(ny * nx, dtype=torch.complex128, device=dev)
     L = _lib.lib()
-    for i, n in enumerate(nv):
-        _lib.check(L.wap_line_transfer(_lib.WAP_TF_ANGULAR, ny * nx, _ptr(kp2), float(n) * float(k0), float(dz),
-                                       _ptr(H), _stream()))
-        Hh, Hl = split_transfer(H.view(ny, nx), dev, cache=False)
-        _lib.check(L.wap_spectrum_propagate(plan.handle, _ptr(X), 1, _ptr(Hh), _ptr(Hl), _ptr(out[i]), _stream()))
+    cur = plan.begin()
+    st = ctypes.c_void_p(cur.cuda_stream)
+    try:
+        for i, n in enumerate(nv):
+            _lib.check(L.wap_line_transfer(_lib.WAP_TF_ANGULAR, ny * nx, _ptr(kp2), float(n) * float(k0),
+                                           float(dz), _ptr(H), st))
+            Hh, Hl = split_transfer(H.view(ny, nx), dev, cache=False)
+            _lib.check(L.wap_spectrum_propagate(plan.handle, _ptr(X), 1, _ptr(Hh), _ptr(Hl), _ptr(out[i]), st))
+    finally:
+        plan.end(cur)
     return out
 
 
@@ -713,8 +772,11 @@ def aperture_probe(ny: int, nx: int, sampling, energy: float, alpha_mrad: float,
     ps_y, ps_x = _pair(sampling)
     plan = get_plan(int(ny), int(nx), 1, _lib.WAP_OP_FRESNEL_AS)
     out = torch.empty((int(ny), int(nx)), dtype=torch.complex64, device=dev)
+    cur = plan.begin()
     _lib.check(_lib.lib().wap_aperture_probe(plan.handle, ps_y, ps_x, float(energy), float(alpha_mrad),
-                                             float(defocus), 1 if centred else 0, _ptr(out), _stream()))
+                                             float(defocus), 1 if centred else 0, _ptr(out),
+                                             ctypes.c_void_p(cur.cuda_stream)))
+    plan.end(cur)
     return out
 
 

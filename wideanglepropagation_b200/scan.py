@@ -77,9 +77,11 @@ def _fwd(c: DeviceClass, b0: int, nb: int) -> None:
     dp = ctypes.c_void_p(c.dp.data_ptr() + b0 * plane * 4)
     pos = ctypes.c_void_p(c.positions.data_ptr() + b0 * 8)
     dr = ctypes.c_void_p(c.draw.data_ptr() + b0 * 4)
+    cur = plan.begin()
     _lib.check(_lib.lib().wap_multislice_fwd(
         plan.handle, _ptr(c.V), c.n_slices, c.n_draws, dr, _ptr(c.probe), nb, 0, pos, _ptr(c.H), _ptr(c.H_lo),
-        c.dz, c.energy, ex, dp, None, _stream()))
+        c.dz, c.energy, ex, dp, None, ctypes.c_void_p(cur.cuda_stream)))
+    plan.end(cur)
 
 
 def launches_per_step(classes: List[DeviceClass], mode: str) -> int:
