@@ -210,7 +210,7 @@ def test_autograd_raises_on_scheduler_timeout(wap):
     g0 = step()
     torch.cuda.synchronize()
     key = (torch.cuda.current_device(), 128, host.n_slices, 1, host.n_probes, 2)
-    h = A._pool[key][-1]
+    h, _ = A._pool[key][-1]   # (scan handle, StreamOrder)
     L = _lib.lib()
     try:
         _lib.check(L.wap_scan_debug_stall(h, 1, 1 << 12))
