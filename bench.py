@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--profile-cluster", action="store_true",
                     help="cluster-kernel case for ncu captures: one Fresnel probe on 128^2, 20 slices (C1's slice "
                          "count and probe on the grid the cluster kernel serves), two calls")
+    ap.add_argument("--profile-chain", action="store_true",
+                    help="chain-kernel case for ncu captures: C1 (Fresnel 256^2, 20 slices, one probe), two calls")
     ap.add_argument("--table", action="store_true",
                     help="per-configuration table (C1 Fresnel 256^2, C2 AS 1024^2, C3 WPM 512^2; one probe): B200 "
                          "time, CPU FP64/FP32 restatement on a bounded sample, error vs the FP64 oracle at full "
@@ -236,6 +238,9 @@ def main():
         return
     if args.profile_cluster:
         profile_cluster()
+        return
+    if args.profile_chain:
+        profile_chain()
         return
     rank, world, local = dist_env()
     import wideanglepropagation_b200.synthetic as S
@@ -535,6 +540,22 @@ def profile_cluster():
         wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
     torch.cuda.synchronize()
     print(json.dumps({"profile_cluster": "ok"}))
+
+
+def profile_chain():
+    """C1 (Fresnel 256^2, 20 slices, one probe) through simulate_fresnel_as,
+    two calls: the case of the one-launch cooperative chain kernel."""
+    import torch
+    import wideanglepropagation_b200 as wap
+    w = wap.synthetic.plain_fresnel(0)
+    dev = torch.device("cuda", 0)
+    V = torch.as_tensor(w.potential[0], device=dev)
+    pr = torch.as_tensor(w.probe, device=dev)
+    H = wap.fresnel_propagation_kernel(w.ny, w.nx, (w.ps, w.ps), w.dz, w.energy)
+    for _ in range(2):
+        wap.simulate_fresnel_as(V, pr, H, w.dz, w.energy, return_wavefronts=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_chain": "ok"}))
 
 
 def baseline_table():
