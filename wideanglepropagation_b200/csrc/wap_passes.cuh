@@ -541,20 +541,32 @@ struct WpmBinsArgs {
 };
 
 // one CTA per (slice, draw): min/max of delta over the slice, then the K
-// reference values delta_min + (delta_max - delta_min) t_k^p in float64
+// reference values delta_min + (delta_max - delta_min) t_k^p in float64.
+// Each thread keeps eight 16-byte loads in flight per trip: with one, the
+// slice's reduction is a chain of 64 memory latencies at 512^2.
 static __global__ void __launch_bounds__(1024) wpm_bins_kernel(const WpmBinsArgs a) {
+  constexpr int kInFlight = 8;
   const int s = blockIdx.x, d = blockIdx.y;
-  const float* vs = a.V + ((long long)d * a.n_slices + s) * a.n_px;
+  const float4* v4 = reinterpret_cast<const float4*>(a.V + ((long long)d * a.n_slices + s) * a.n_px);
+  const int n4 = a.n_px >> 2, step = blockDim.x;
   float lo = 3.0e38f, hi = -3.0e38f;
-  for (int i = threadIdx.x * 4; i < a.n_px; i += blockDim.x * 4) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(vs + i));
+  auto fold = [&](const float4 q) {
     const float d0 = refr_minus_one(q.x, a.ri_a, a.ri_inv_den);
     const float d1 = refr_minus_one(q.y, a.ri_a, a.ri_inv_den);
     const float d2 = refr_minus_one(q.z, a.ri_a, a.ri_inv_den);
     const float d3 = refr_minus_one(q.w, a.ri_a, a.ri_inv_den);
     lo = fminf(lo, fminf(fminf(d0, d1), fminf(d2, d3)));
     hi = fmaxf(hi, fmaxf(fmaxf(d0, d1), fmaxf(d2, d3)));
+  };
+  int i = threadIdx.x;
+  for (; i + (kInFlight - 1) * step < n4; i += kInFlight * step) {
+    float4 q[kInFlight];
+#pragma unroll
+    for (int u = 0; u < kInFlight; ++u) q[u] = __ldg(v4 + i + u * step);
+#pragma unroll
+    for (int u = 0; u < kInFlight; ++u) fold(q[u]);
   }
+  for (; i < n4; i += step) fold(__ldg(v4 + i));
   __shared__ float slo[32], shi[32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
