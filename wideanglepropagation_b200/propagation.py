@@ -27,7 +27,7 @@ from __future__ import annotations
 import ctypes
 import math
 import threading
-from typing import Optional, Sequence
+from typing import Optional
 
 import numpy as np
 import torch
